@@ -1,0 +1,235 @@
+"""CPU oracle bindings -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module.  It exposes
+
+* the C restatement ``liblbmoracle.so`` (lbm_oracle.c) through ctypes, and
+* ``run_reference``: the reference's own unmodified step functions, compiled
+  into ``oracle/_ref/dnsref`` (ref_harness.c), run as a subprocess in a
+  scratch directory, with the log files they write parsed back.
+
+State layout everywhere: the reference's lbf/ftemp layout without ghosts,
+``state[x, y, z, a]`` float64 with shape (nx, ny, nz+2, 19); z=0 and z=nz+1 are
+the wall planes.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbmoracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "dnsref")
+
+LOG_NAMES = ("force", "rho", "energy", "flowrate", "massrate", "stup", "stdown", "stress", "pgrad")
+NLOG = len(LOG_NAMES)
+
+_lib = None
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the restatement (always) and the reference harness (when the
+    reference sources are present on this machine)."""
+    out = subprocess.DEVNULL if quiet else None
+    subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=out)
+    if os.path.isdir("/root/reference/DNS-solver/src"):
+        subprocess.run(["make", "-C", HERE, "ref"], check=True, stdout=out)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        i8p = ctypes.POINTER(ctypes.c_int8)
+        ci, cd, cl = ctypes.c_int, ctypes.c_double, ctypes.c_long
+        L.orc_step.argtypes = [ci, ci, ci, dp, dp, i8p, cd, cd, ci]
+        L.orc_encalc.argtypes = [ci, ci, ci, dp, cd, dp]
+        L.orc_encalc.restype = cd
+        L.orc_wshearstr.argtypes = [ci, ci, ci, dp, cd, cd, dp]
+        L.orc_statistics.argtypes = [ci, ci, ci, dp, dp]
+        L.orc_moments.argtypes = [ci, ci, ci, dp, dp, dp]
+        L.orc_run.argtypes = [ci, ci, ci, dp, i8p, cd, cd, cd, ci, cl, dp, ci]
+        L.orc_run.restype = cl
+        L.orc_flags_smooth.argtypes = [ci, ci, ci, i8p]
+        L.orc_flags_ridges.argtypes = [ci, ci, ci, ci, ci, i8p]
+        L.orc_flags_transverse.argtypes = [ci, ci, ci, ci, ci, i8p]
+        L.orc_flags_posts.argtypes = [ci, ci, ci, ci, ci, ci, ci, i8p]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i8(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int8))
+
+
+def _dims(state):
+    nx, ny, zd, q = state.shape
+    assert q == 19 and state.dtype == np.float64 and state.flags.c_contiguous
+    return nx, ny, zd - 2
+
+
+# ---------------------------------------------------------------- flags
+def flags(kind: str, nx: int, ny: int, nz: int, **kw) -> np.ndarray:
+    """Periodic-grid flags (nx, ny, nz+2) int8: 0 fluid, -1 no-slip, -2 slip."""
+    f = np.zeros((nx, ny, nz + 2), np.int8)
+    L = lib()
+    if kind == "smooth":
+        L.orc_flags_smooth(nx, ny, nz, _i8(f))
+    elif kind == "ridges":
+        L.orc_flags_ridges(nx, ny, nz, kw.get("gap", 2), kw.get("width", 2), _i8(f))
+    elif kind == "transverse":
+        L.orc_flags_transverse(nx, ny, nz, kw.get("gap", 2), kw.get("width", 2), _i8(f))
+    elif kind == "posts":
+        L.orc_flags_posts(nx, ny, nz, kw.get("gx", 2), kw.get("wx", 2), kw.get("gy", 2), kw.get("wy", 2), _i8(f))
+    else:
+        raise ValueError(kind)
+    return f
+
+
+# ---------------------------------------------------------------- restatement
+def run(state, flg, omega, ubulk=0.0, gx=0.0, const_g=True, nsteps=1, bc_mode=0):
+    """Advance ``state`` (modified in place) nsteps; returns logs (nsteps, 9)."""
+    nx, ny, nz = _dims(state)
+    flg = np.ascontiguousarray(flg, np.int8)
+    logs = np.zeros((nsteps, NLOG), np.float64)
+    done = lib().orc_run(nx, ny, nz, _dp(state), _i8(flg), omega, ubulk, gx, int(const_g), nsteps, _dp(logs), bc_mode)
+    if done != nsteps:
+        raise FloatingPointError(f"oracle stopped after {done} of {nsteps} steps (NaN wall stress)")
+    return logs
+
+
+def step(state, flg, omega, force, bc_mode=0):
+    nx, ny, nz = _dims(state)
+    scratch = state.copy()
+    lib().orc_step(nx, ny, nz, _dp(state), _dp(scratch), _i8(np.ascontiguousarray(flg, np.int8)), omega, force, bc_mode)
+
+
+def encalc(state, ubulk):
+    nx, ny, nz = _dims(state)
+    out = np.zeros(NLOG)
+    force = lib().orc_encalc(nx, ny, nz, _dp(state), ubulk, _dp(out))
+    out[0] = force
+    return out
+
+
+def wshearstr(state, omega, force):
+    nx, ny, nz = _dims(state)
+    out = np.zeros(NLOG)
+    lib().orc_wshearstr(nx, ny, nz, _dp(state), omega, force, _dp(out))
+    return out
+
+
+def statistics(state):
+    nx, ny, nz = _dims(state)
+    out = np.zeros(9 * (nz + 2))
+    lib().orc_statistics(nx, ny, nz, _dp(state), _dp(out))
+    return out.reshape(9, nz + 2)
+
+
+def moments(state):
+    nx, ny, nz = _dims(state)
+    vel = np.zeros((nx, ny, nz + 2, 3))
+    den = np.zeros((nx, ny, nz + 2))
+    lib().orc_moments(nx, ny, nz, _dp(state), _dp(vel), _dp(den))
+    return vel, den
+
+
+# ---------------------------------------------------------------- reference
+def have_reference() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+def ghost_flags(flg: np.ndarray) -> np.ndarray:
+    """Periodic-grid flags -> the reference's int32 s-array [xd][yd][zd] with
+    ghost planes (flag 1 on the fluid part of the i/j edge planes, exactly as
+    solid_init.c:30-45 sets them; wall planes copied periodically)."""
+    nx, ny, zd = flg.shape
+    s = np.zeros((nx + 1, ny + 1, zd), np.int32)
+    s[:nx, :ny] = flg
+    s[nx, :ny] = flg[0]
+    s[:nx, ny] = flg[:, 0]
+    s[nx, ny] = flg[0, 0]
+    fluid = s[:, :, 1:zd - 1] >= 0
+    edge = np.zeros_like(fluid)
+    edge[0], edge[nx] = True, True
+    edge[:, 0], edge[:, ny] = True, True
+    s[:, :, 1:zd - 1][fluid & edge] = 1
+    return s
+
+
+def _parse_log(path):
+    if not os.path.exists(path):
+        return None
+    return np.loadtxt(path, ndmin=2)[:, 1]
+
+
+def run_reference(state, omega, ubulk=0.0, gx=0.0, const_g=True, nsteps=1, texture="smooth",
+                  flags_periodic=None, stats_every=0, vel_every=0, timeout=600):
+    """Run the reference's own step functions.  Returns dict with 'state',
+    'force'/'rho' (full precision, per step), the parsed text logs, and
+    statistics / vel / den arrays when requested."""
+    if not have_reference():
+        raise FileNotFoundError(REF_BIN)
+    nx, ny, nz = _dims(state)
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "in.bin")
+        state.tofile(inp)
+        args = [REF_BIN, f"xdv={nx}", f"ydv={ny}", f"zdv={nz}", f"omega={omega!r}", f"ubulk={ubulk!r}",
+                f"mode={'g' if const_g else 'q'}", f"gx={gx!r}", f"steps={nsteps}", "in=in.bin",
+                "out=out.bin", "force_out=force.bin", f"stats_every={stats_every}", f"vel_every={vel_every}"]
+        if flags_periodic is not None:
+            ghost_flags(flags_periodic).tofile(os.path.join(td, "flags.bin"))
+            args += ["texture=file", "flags=flags.bin"]
+        else:
+            args += [f"texture={texture}"]
+        subprocess.run(args, cwd=td, check=True, timeout=timeout, stdout=subprocess.DEVNULL)
+        res = {"state": np.fromfile(os.path.join(td, "out.bin")).reshape(state.shape)}
+        fr = np.fromfile(os.path.join(td, "force.bin")).reshape(-1, 2)
+        res["force"], res["rho"] = fr[:, 0], fr[:, 1]
+        for name, fn in (("energy", "energy.txt"), ("flowrate", "flowrate.txt"), ("massrate", "massrate.txt"),
+                         ("stup", "str-up.txt"), ("stdown", "str-do.txt"), ("stress", "w-str.txt"),
+                         ("pgrad", "p-grad.txt")):
+            res[name] = _parse_log(os.path.join(td, fn))
+        if stats_every:
+            res["stats"] = [np.fromfile(os.path.join(td, f"turb-fld.000.{t:03d}")).reshape(9, nz + 2)
+                            for t in range((nsteps - 1) // stats_every + 1)]
+        if vel_every:
+            res["vel"] = [np.fromfile(os.path.join(td, f"vel.{t:04d}")).reshape(nx, ny, nz + 2, 3)
+                          for t in range((nsteps - 1) // vel_every + 1)]
+            res["den"] = [np.fromfile(os.path.join(td, f"den.{t:04d}")).reshape(nx, ny, nz + 2)
+                          for t in range((nsteps - 1) // vel_every + 1)]
+        return res
+
+
+def time_reference(nx, ny, nz, nsteps, omega=1.9, ubulk=0.05, procs=1, timeout=900):
+    """CPU baseline: ``procs`` independent single-rank reference processes,
+    each advancing its own x-slab (nx//procs cells) as its own periodic box
+    from the reference's rest state.  Returns (aggregate MLUPS, wall seconds)."""
+    import time
+    slab = max(nx // procs, 4)
+    with tempfile.TemporaryDirectory() as td:
+        t0 = time.perf_counter()
+        ps = []
+        for p in range(procs):
+            d = os.path.join(td, str(p))
+            os.makedirs(d)
+            ps.append(subprocess.Popen([REF_BIN, f"xdv={slab}", f"ydv={ny}", f"zdv={nz}", f"omega={omega!r}",
+                                        f"ubulk={ubulk!r}", "mode=q", f"steps={nsteps}", "time=1"],
+                                       cwd=d, stdout=subprocess.PIPE, text=True))
+        outs = [p.communicate(timeout=timeout)[0] for p in ps]
+        wall = time.perf_counter() - t0
+    if any(p.returncode for p in ps):
+        raise RuntimeError("reference process failed")
+    cells = float(slab) * ny * nz * nsteps * procs
+    return cells / wall / 1e6, wall
