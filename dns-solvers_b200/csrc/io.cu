@@ -1,0 +1,260 @@
+// State import/export in the reference's AoS lbf layout, per-cell moments
+// (vel_print.c) and the two-pass plane statistics (statistics.c), for every
+// storage precision and either AA parity.
+//
+// After an even step the populations sit post-collision in swapped slots; the
+// natural (post-stream) value f_a of a cell is then what the odd step would
+// load into f[a], so every reader here gathers through the odd address set.
+#include <cuda_fp16.h>
+
+#include "step_common.cuh"
+
+namespace dnslbm {
+
+template <typename T> struct Nat;
+template <> struct Nat<double> {
+    static __device__ __forceinline__ double ld(const double *p, int) { return *p; }
+    static __device__ __forceinline__ void st(double *p, double f, int) { *p = f; }
+};
+template <> struct Nat<float> {
+    static __device__ __forceinline__ double ld(const float *p, int a) { return wq(a) + (double)*p; }
+    static __device__ __forceinline__ void st(float *p, double f, int a) { *p = (float)(f - wq(a)); }
+    static __device__ __forceinline__ double wq(int a) { return a == 0 ? 1. / 3. : a <= 6 ? 1. / 18. : 1. / 36.; }
+};
+template <> struct Nat<__half> {
+    static __device__ __forceinline__ double ld(const __half *p, int a)
+    {
+        return Nat<float>::wq(a) + (double)__half2float(*p) * (1. / 32768.);
+    }
+    static __device__ __forceinline__ void st(__half *p, double f, int a)
+    {
+        *p = __double2half((f - Nat<float>::wq(a)) * 32768.);
+    }
+};
+
+template <typename T, int A>
+__device__ __forceinline__ double gather_one(const IoArgs &p, const Nbr &n, int wall, unsigned bits)
+{
+    int slot, idx;
+    aa_address<A, true>(n, wall, bits, slot, idx);
+    return Nat<T>::ld(static_cast<const T *>(p.pop[slot]) + idx, lat_opp(A));
+}
+
+// natural populations of cell (x, y, z)
+template <typename T>
+__device__ __forceinline__ void gather_natural(const IoArgs &p, int x, int y, int z, double (&f)[Q])
+{
+    if (!p.odd) {
+        const int c = (z * p.ny + y) * p.nx + x;
+#pragma unroll
+        for (int a = 0; a < Q; ++a) f[a] = Nat<T>::ld(static_cast<const T *>(p.pop[a]) + c, a);
+        return;
+    }
+    const Nbr n = make_nbr(x, y, z, p.nx, p.ny);
+    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    unsigned bits = 0x1fu;
+    if (p.textured && wall != 0) bits = p.wallmask[(size_t)(wall > 0) * p.nx * p.ny + y * p.nx + x];
+#pragma unroll
+    for (int a = 0; a < Q; ++a) {
+        double v;
+        switch (a) {
+#define G1(A) case A: v = gather_one<T, A>(p, n, wall, bits); break;
+            G1(0) G1(1) G1(2) G1(3) G1(4) G1(5) G1(6) G1(7) G1(8) G1(9)
+            G1(10) G1(11) G1(12) G1(13) G1(14) G1(15) G1(16) G1(17) G1(18)
+#undef G1
+        }
+        f[lat_opp(a)] = v;
+    }
+}
+
+// cells of x-slab [x0, x0+nxc), one thread per fluid cell; AoS index
+// ((x-x0)*ny + y)*zd + (z+1)
+template <typename T>
+__global__ void export_kernel(const IoArgs p, int x0, int nxc, double *aos)
+{
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ncell = (long long)nxc * p.ny * p.nz;
+    if (tid >= ncell) return;
+    const int z = (int)(tid % p.nz);
+    const int y = (int)((tid / p.nz) % p.ny);
+    const int xl = (int)(tid / ((long long)p.nz * p.ny));
+    double f[Q];
+    gather_natural<T>(p, x0 + xl, y, z, f);
+    double *o = aos + (((size_t)xl * p.ny + y) * (p.nz + 2) + (z + 1)) * Q;
+#pragma unroll
+    for (int a = 0; a < Q; ++a) o[a] = f[a];
+}
+
+template <typename T>
+__global__ void import_kernel(const IoArgs p, int x0, int nxc, const double *aos)
+{
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ncell = (long long)nxc * p.ny * p.nz;
+    if (tid >= ncell) return;
+    const int z = (int)(tid % p.nz);
+    const int y = (int)((tid / p.nz) % p.ny);
+    const int xl = (int)(tid / ((long long)p.nz * p.ny));
+    const double *i = aos + (((size_t)xl * p.ny + y) * (p.nz + 2) + (z + 1)) * Q;
+    const int c = (z * p.ny + y) * p.nx + (x0 + xl);
+#pragma unroll
+    for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, i[a], a);
+}
+
+// rest state f = w (init.c:6-19)
+template <typename T>
+__global__ void rest_kernel(const IoArgs p)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long long)p.nx * p.ny * p.nz) return;
+#pragma unroll
+    for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, Nat<float>::wq(a), a);
+}
+
+// vel_print.c:71-96: moments in the reference's order, u = 0, rho = 0 where
+// rho <= 0; wall planes are written as zeros.
+template <typename T>
+__global__ void moments_kernel(const IoArgs p, int x0, int nxc, double *vel, double *den)
+{
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int zd = p.nz + 2;
+    const long long ncell = (long long)nxc * p.ny * zd;
+    if (tid >= ncell) return;
+    const int k = (int)(tid % zd);
+    const int y = (int)((tid / zd) % p.ny);
+    const int xl = (int)(tid / ((long long)zd * p.ny));
+    double ux = 0., uy = 0., uz = 0., dens = 0.;
+    if (k >= 1 && k <= p.nz) {
+        double f[Q];
+        gather_natural<T>(p, x0 + xl, y, k - 1, f);
+#pragma unroll
+        for (int a = 0; a < Q; ++a) {
+            if (lat_ex(a) > 0) ux = ux + f[a];
+            if (lat_ex(a) < 0) ux = ux - f[a];
+            if (lat_ey(a) > 0) uy = uy + f[a];
+            if (lat_ey(a) < 0) uy = uy - f[a];
+            if (lat_ez(a) > 0) uz = uz + f[a];
+            if (lat_ez(a) < 0) uz = uz - f[a];
+            dens = dens + f[a];
+        }
+        if (dens > 0.) {
+            ux /= dens;
+            uy /= dens;
+            uz /= dens;
+        } else {
+            ux = 0.; uy = 0.; uz = 0.; dens = 0.;
+        }
+    }
+    const size_t o = ((size_t)xl * p.ny + y) * zd + k;
+    if (vel) {
+        vel[o * 3 + 0] = ux;
+        vel[o * 3 + 1] = uy;
+        vel[o * 3 + 2] = uz;
+    }
+    if (den) den[o] = dens;
+}
+
+// Two-pass plane statistics (statistics.c:31-132).  pass 0: sums of
+// u, v, w, rho per plane; pass 1: sums of u'^2, v'^2, w'^2, u'w', rho'^2
+// about the plane means `mean` [nz][4].  Block partials [nz][bpp][5].
+constexpr int NS = 5;
+template <typename T>
+__global__ void __launch_bounds__(128) stats_kernel(const IoArgs p, int rows, int pass, const double *mean,
+                                                    double *partials)
+{
+    __shared__ double smem[32 * NS];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.z;
+    double acc[NS] = {0, 0, 0, 0, 0};
+    if (x < p.nx) {
+        const int y0 = blockIdx.y * rows, y1 = min(y0 + rows, p.ny);
+        for (int y = y0; y < y1; ++y) {
+            double f[Q];
+            gather_natural<T>(p, x, y, z, f);
+            double dens = 0., u = 0., v = 0., w = 0.;
+#pragma unroll
+            for (int a = 0; a < Q; ++a) {
+                dens = dens + f[a];
+                if (lat_ex(a) > 0) u = u + f[a];
+                if (lat_ex(a) < 0) u = u - f[a];
+                if (lat_ey(a) > 0) v = v + f[a];
+                if (lat_ey(a) < 0) v = v - f[a];
+                if (lat_ez(a) > 0) w = w + f[a];
+                if (lat_ez(a) < 0) w = w - f[a];
+            }
+            if (pass == 0) {
+                acc[0] += u / dens;
+                acc[1] += v / dens;
+                acc[2] += w / dens;
+                acc[3] += dens;
+            } else {
+                const double uf = (u / dens) - mean[z * 4 + 0], vf = (v / dens) - mean[z * 4 + 1];
+                const double wf = (w / dens) - mean[z * 4 + 2], df = dens - mean[z * 4 + 3];
+                acc[0] += uf * uf;
+                acc[1] += vf * vf;
+                acc[2] += wf * wf;
+                acc[3] += uf * wf;
+                acc[4] += df * df;
+            }
+        }
+    }
+    block_sum<NS>(acc, smem);
+    if (threadIdx.x == 0) {
+        const unsigned bpp = gridDim.x * gridDim.y;
+        double *o = partials + ((size_t)z * bpp + blockIdx.y * gridDim.x + blockIdx.x) * NS;
+#pragma unroll
+        for (int i = 0; i < NS; ++i) o[i] = acc[i];
+    }
+}
+
+// one block per plane: fixed-order sum of the plane's block partials
+__global__ void plane_reduce_kernel(const double *partials, int bpp, double *out /* [nz][NS] */)
+{
+    __shared__ double smem[32 * NS];
+    const int z = blockIdx.x;
+    double s[NS] = {0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < bpp; b += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < NS; ++i) s[i] += partials[((size_t)z * bpp + b) * NS + i];
+    block_sum<NS>(s, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int i = 0; i < NS; ++i) out[z * NS + i] = s[i];
+}
+
+// ---------------------------------------------------------------- launchers
+template <typename T>
+static void io_dispatch(int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s)
+{
+    const int bs = 256;
+    if (what == 0) {
+        const long long n = (long long)nxc * p.ny * p.nz;
+        export_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p, x0, nxc, a);
+    } else if (what == 1) {
+        const long long n = (long long)nxc * p.ny * p.nz;
+        import_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p, x0, nxc, a);
+    } else if (what == 2) {
+        const long long n = (long long)p.nx * p.ny * p.nz;
+        rest_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p);
+    } else {
+        const long long n = (long long)nxc * p.ny * (p.nz + 2);
+        moments_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p, x0, nxc, a, b);
+    }
+}
+
+void launch_io(int precision, int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s)
+{
+    if (precision == 64) io_dispatch<double>(what, p, x0, nxc, a, b, s);
+    else if (precision == 32) io_dispatch<float>(what, p, x0, nxc, a, b, s);
+    else io_dispatch<__half>(what, p, x0, nxc, a, b, s);
+}
+
+void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int rows, int pass, const double *mean,
+                  double *partials, double *plane_out, cudaStream_t s)
+{
+    if (precision == 64) stats_kernel<double><<<grid, block, 0, s>>>(p, rows, pass, mean, partials);
+    else if (precision == 32) stats_kernel<float><<<grid, block, 0, s>>>(p, rows, pass, mean, partials);
+    else stats_kernel<__half><<<grid, block, 0, s>>>(p, rows, pass, mean, partials);
+    plane_reduce_kernel<<<p.nz, 128, 0, s>>>(partials, (int)(grid.x * grid.y), plane_out);
+}
+
+}  // namespace dnslbm

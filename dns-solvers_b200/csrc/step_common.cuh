@@ -1,0 +1,249 @@
+// Shared machinery of the fused step kernels: launch arguments, the AA
+// address set of a cell (with periodic wrap and wall links), the
+// deterministic block/plane/grid reduction, and the per-step tail that turns
+// per-plane sums into the encalc/wshearstr log record and the next force.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lattice.cuh"
+
+namespace dnslbm {
+
+// Per-block partial sums.  Reader side (state at the start of the step):
+//   0 sum rho, 1 sum jx (raw momentum), 2..4 sum u,v,w (u = j/rho),
+//   5 sum |u - c(z)|^2 with c(z) the previous plane means (a shift that keeps
+//     the one-pass variance free of cancellation).
+// Writer side (state after the step, constant-Q only):
+//   6 sum of post-collision populations, 7 their x-momentum as received
+//     (bounce-back flips e_x, specular reflection keeps it).
+constexpr int NP = 8;
+
+struct StepArgs {
+    void *pop[Q];            // population arrays (slot a)
+    int nx, ny, nz;
+    int rows;                // rows (y) per block
+    const uint8_t *wallmask; // [2][ny][nx] wall-link bits (bottom, top)
+    double omega, ubulk, gx;
+    int const_q;
+    double *force;           // [2] force of step s is force[s & 1]
+    double *shift;           // [2][nz][3] plane means of the previous state
+    long long *step_ctr;     // steps done (advanced by the step tail)
+    double *partials;        // [blocks][NP]
+    double *plane_sums;      // [nz][NP]
+    unsigned *plane_ctr;     // [nz]
+    unsigned *total_ctr;     // [1]
+    double *logs;            // [log_cap][9]
+    int log_cap;
+    long long *status;       // [0] first NaN step + 1 (0: none)
+};
+
+// Arguments of the state readers/writers (import, export, moments, stats).
+struct IoArgs {
+    void *pop[Q];
+    int nx, ny, nz;
+    const uint8_t *wallmask;
+    int textured;
+    int odd;  // 1: populations are post-collision in swapped slots
+};
+
+// ---------------------------------------------------------------- addresses
+// Neighbourhood of a cell: wrapped x and the 9 row offsets (dy, dz).
+struct Nbr {
+    int x, xm, xp;
+    int row[3][3];  // row[dy+1][dz+1] = ((z+dz)*ny + wrap(y+dy))*nx
+    int c0;         // own cell
+};
+
+__device__ __forceinline__ Nbr make_nbr(int x, int y, int z, int nx, int ny)
+{
+    Nbr n;
+    n.x = x;
+    n.xm = x == 0 ? nx - 1 : x - 1;
+    n.xp = x == nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? ny - 1 : y - 1;
+    const int yp = y == ny - 1 ? 0 : y + 1;
+    const int ys[3] = {ym, y, yp};
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz) n.row[dy][dz] = ((z + dz - 1) * ny + ys[dy]) * nx;
+    n.c0 = n.row[1][1] + x;
+    return n;
+}
+
+__device__ __forceinline__ int nbr_x(const Nbr &n, int ex) { return ex == 0 ? n.x : ex > 0 ? n.xp : n.xm; }
+
+// Element index (within population array `slot`) of the A-th address of the
+// cell, and the slot it lives in.
+//   even: slot A at the cell; load -> f[A], store <- f*[opp A]
+//   odd:  slot A at cell + e_A; load -> f[opp A], store <- f*[A]
+// Odd step, wall plane, A pointing into the wall: bounce-back uses slot
+// opp(A) at the cell, specular reflection slot mirror(A) at the tangential
+// neighbour (cell + (ex, ey, 0)).  `wall` is -1 (bottom plane), +1 (top
+// plane) or 0; `bits` are the cell's wall-link bits.
+template <int A, bool ODD>
+__device__ __forceinline__ void aa_address(const Nbr &n, int wall, unsigned bits, int &slot, int &idx)
+{
+    constexpr int ex = lat_ex(A), ey = lat_ey(A), ez = lat_ez(A);
+    if (!ODD || A == 0) {
+        slot = A;
+        idx = n.c0;
+        return;
+    }
+    if (ez != 0 && wall == ez) {
+        if ((bits >> wall_link(A)) & 1u) {
+            slot = lat_opp(A);
+            idx = n.c0;
+        } else {
+            slot = lat_mir(A);
+            idx = n.row[ey + 1][1] + nbr_x(n, ex);
+        }
+        return;
+    }
+    slot = A;
+    idx = n.row[ey + 1][ez + 1] + nbr_x(n, ex);
+}
+
+// ---------------------------------------------------------------- reduction
+template <int NV>
+__device__ __forceinline__ void warp_sum(double (&v)[NV])
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
+}
+
+// Deterministic block sum (fixed shuffle tree, warps added in order); the
+// result is valid in thread 0.  smem holds 32*NV doubles.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarp = (blockDim.x + 31) >> 5;
+    warp_sum<NV>(v);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) smem[warp * NV + i] = v[i];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] = lane < nwarp ? smem[lane * NV + i] : 0.0;
+        warp_sum<NV>(v);
+    }
+}
+
+// Final step tail, run by the last block of the launch: plane sums ->
+// per-step log record, the plane means (next TKE shift) and, in constant-Q
+// mode, the force of the next step from the writer-side totals.
+// mode 0: after a step (logs, advances the step counter);
+// mode 1: initial reduction of a freshly loaded state (force and shift of
+//         the current step from the reader-side totals, nothing logged).
+static __device__ __forceinline__ void step_tail(const StepArgs &a, long long step, double force_used, int mode, double *smem)
+{
+    const int nz = a.nz;
+    const double np = (double)a.nx * (double)a.ny;
+    const double *cshift = a.shift + (size_t)(step & 1) * nz * 3;
+    double *nshift = a.shift + (size_t)((mode == 0 ? step + 1 : step) & 1) * nz * 3;
+    double t[6] = {0, 0, 0, 0, 0, 0};  // rho, jx, sum of plane means u, K, writer rho, writer jx
+    for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+        const double *ps = a.plane_sums + (size_t)z * NP;
+        double s[NP];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) s[i] = __ldcg(ps + i);
+        const double um = s[2] / np, vm = s[3] / np, wm = s[4] / np;
+        const double du = um - cshift[z * 3 + 0], dv = vm - cshift[z * 3 + 1], dw = wm - cshift[z * 3 + 2];
+        t[0] += s[0];
+        t[1] += s[1];
+        t[2] += um;
+        t[3] += 0.5 * (s[5] - np * (du * du + dv * dv + dw * dw));
+        t[4] += s[6];
+        t[5] += s[7];
+        nshift[z * 3 + 0] = um;
+        nshift[z * 3 + 1] = vm;
+        nshift[z * 3 + 2] = wm;
+    }
+    block_sum<6>(t, smem);
+    if (threadIdx.x != 0) return;
+    const double N = np * (double)nz;
+    const double rho = t[0] / N, momentum = t[1] / N;
+    if (mode == 1) {
+        a.force[step & 1] = a.const_q ? rho * a.ubulk - momentum : a.gx;
+        return;
+    }
+    // wall shear stress, wshearstr.c:24-121 (top density from plane zd-4)
+    auto umean = [&](int z) { return __ldcg(a.plane_sums + (size_t)z * NP + 2) / np; };
+    const double mu = (1. / 6.) * (2. / a.omega - 1);
+    const double davg_dn = __ldcg(a.plane_sums + 0 * NP + 0) / np;
+    const double davg_up = __ldcg(a.plane_sums + (size_t)(nz - 3) * NP + 0) / np;
+    double stdown = -2. * umean(0) + 3. * umean(1) - umean(2);
+    double stup = -(2. * umean(nz - 1) - 3. * umean(nz - 2) + umean(nz - 3));
+    stdown *= mu * davg_dn;
+    stup *= mu * davg_up;
+    const double stress = 0.5 * (stup + stdown);
+    double *rec = a.logs + (size_t)(step % a.log_cap) * 9;
+    rec[0] = force_used;
+    rec[1] = rho;
+    rec[2] = t[3] / N;
+    rec[3] = (t[2] / (double)nz) * (double)(a.ny * nz);
+    rec[4] = momentum * (double)(a.ny * nz);
+    rec[5] = stup;
+    rec[6] = stdown;
+    rec[7] = stress;
+    rec[8] = force_used * nz / 2.;
+    if (stress != stress && a.status[0] == 0) a.status[0] = step + 1;
+    // constant-Q: next force from the totals of the state this step wrote
+    // (encalc.c:121 evaluated one step ahead); sum of populations = t[4]
+    a.force[(step + 1) & 1] = a.const_q ? (t[4] / N) * a.ubulk - t[5] / N : a.gx;
+    *a.step_ctr = step + 1;
+}
+
+// Block epilogue of every fused kernel: block partials -> (last block of the
+// plane) plane sums -> (last plane) step tail.  No block waits for another:
+// the last arrival does the work, found with atomic tickets.
+__device__ __forceinline__ void block_epilogue(const StepArgs &a, double (&acc)[NP], long long step, double force_used,
+                                               int mode)
+{
+    __shared__ double smem[32 * NP];
+    __shared__ unsigned ticket;
+    block_sum<NP>(acc, smem);
+    const unsigned bpp = gridDim.x * gridDim.y;
+    const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const int z = blockIdx.z;
+    if (threadIdx.x == 0) {
+        double *p = a.partials + ((size_t)z * bpp + bid) * NP;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) p[i] = acc[i];
+        __threadfence();
+        ticket = atomicAdd(a.plane_ctr + z, 1u);
+    }
+    __syncthreads();
+    if (ticket != bpp - 1) return;
+    // last block of plane z: fixed-order plane sum
+    __threadfence();
+    double s[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) s[i] = 0.0;
+    for (unsigned b = threadIdx.x; b < bpp; b += blockDim.x) {
+        const double *p = a.partials + ((size_t)z * bpp + b) * NP;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) s[i] += __ldcg(p + i);
+    }
+    block_sum<NP>(s, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) a.plane_sums[(size_t)z * NP + i] = s[i];
+        a.plane_ctr[z] = 0;
+        __threadfence();
+        ticket = atomicAdd(a.total_ctr, 1u);
+    }
+    __syncthreads();
+    if (ticket != (unsigned)a.nz - 1) return;
+    __threadfence();
+    step_tail(a, step, force_used, mode, smem);
+    if (threadIdx.x == 0) *a.total_ctr = 0;
+}
+
+}  // namespace dnslbm

@@ -1,0 +1,216 @@
+"""Python binding of the dnslbm C ABI (include/dnslbm.h) over ctypes.
+
+The product is ``libdnslbm.so`` (sm_100a kernels + C ABI); this module only
+marshals numpy arrays to it.  There is no fallback: if the library or a CUDA
+device is missing, every call raises.
+
+Array layouts are the reference's (see include/dnslbm.h):
+  state  float64 (xdv, ydv, zdv+2, 19)   lbf/ftemp layout without ghosts
+  flags  int8    (xdv, ydv, zdv+2)       0 fluid, -1 no-slip, -2 slip
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdnslbm.so")
+
+OK, ERR_ARG, ERR_CUDA, ERR_NAN, ERR_TIMEOUT, ERR_NOMEM, ERR_IO, ERR_STATE = range(8)
+F64, F32, F16 = 64, 32, 16
+CONST_Q, CONST_G = 0, 1
+BC_REFERENCE, BC_GENERAL = 0, 1
+LOG_NAMES = ("force", "rho", "energy", "flowrate", "massrate", "stup", "stdown", "stress", "pgrad")
+
+
+class DnsLbmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dnslbm error {code}: {msg}")
+        self.code = code
+
+
+class Deck(ctypes.Structure):
+    """The reference's parameter deck (definitions.h:30-59), at run time."""
+    _fields_ = [("xdv", ctypes.c_int), ("ydv", ctypes.c_int), ("zdv", ctypes.c_int),
+                ("omega", ctypes.c_double), ("ubulk", ctypes.c_double), ("gx", ctypes.c_double),
+                ("force_mode", ctypes.c_int), ("precision", ctypes.c_int), ("bc_mode", ctypes.c_int),
+                ("log_capacity", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libdnslbm.so (raises if it is missing: there is no CPU path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} not built (run __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, ip, i8p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), \
+        ctypes.POINTER(ctypes.c_int8)
+    L.dnslbm_create.argtypes = [ctypes.POINTER(Deck), ctypes.POINTER(vp)]
+    L.dnslbm_destroy.argtypes = [vp]
+    L.dnslbm_destroy.restype = None
+    L.dnslbm_last_error.argtypes = [vp]
+    L.dnslbm_last_error.restype = ctypes.c_char_p
+    L.dnslbm_set_flags.argtypes = [vp, ip]
+    L.dnslbm_set_flags_periodic.argtypes = [vp, i8p]
+    L.dnslbm_init_rest.argtypes = [vp]
+    L.dnslbm_load_state.argtypes = [vp, dp]
+    L.dnslbm_store_state.argtypes = [vp, dp]
+    L.dnslbm_step.argtypes = [vp, ctypes.c_long]
+    L.dnslbm_steps_done.argtypes = [vp]
+    L.dnslbm_steps_done.restype = ctypes.c_long
+    L.dnslbm_logs.argtypes = [vp, ctypes.c_long, ctypes.c_long, dp]
+    L.dnslbm_get_force.argtypes = [vp, dp]
+    L.dnslbm_statistics.argtypes = [vp, dp]
+    L.dnslbm_moments.argtypes = [vp, dp, dp]
+    L.dnslbm_step_timed.argtypes = [vp, ctypes.c_long, dp, dp, dp]
+    L.dnslbm_bytes_per_cell.argtypes = [vp]
+    L.dnslbm_bytes_per_cell.restype = ctypes.c_double
+    L.dnslbm_sync.argtypes = [vp]
+    L.dnslbm_host_alloc.argtypes = [ctypes.c_size_t]
+    L.dnslbm_host_alloc.restype = vp
+    L.dnslbm_host_free.argtypes = [vp]
+    L.dnslbm_host_free.restype = None
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Channel:
+    """One channel on one GPU: a dnslbm context."""
+
+    def __init__(self, xdv, ydv, zdv, omega, ubulk=0.0, gx=0.0, force_mode=CONST_G, precision=F64,
+                 bc_mode=BC_REFERENCE, log_capacity=0, device=0):
+        self.L = lib()
+        self.shape = (xdv, ydv, zdv)
+        d = Deck(xdv, ydv, zdv, omega, ubulk, gx, force_mode, precision, bc_mode, log_capacity, device)
+        h = ctypes.c_void_p()
+        rc = self.L.dnslbm_create(ctypes.byref(d), ctypes.byref(h))
+        if rc:
+            raise DnsLbmError(rc, self.L.dnslbm_last_error(None).decode())
+        self.h = h
+        self.deck = d
+
+    def _ck(self, rc):
+        if rc:
+            raise DnsLbmError(rc, self.L.dnslbm_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.dnslbm_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def state_shape(self):
+        x, y, z = self.shape
+        return (x, y, z + 2, 19)
+
+    def set_flags(self, flags):
+        """flags: int8 (xdv, ydv, zdv+2) periodic grid, or int32 reference
+        V.s array (xdv+1, ydv+1, zdv+2) with ghost planes."""
+        if flags.dtype == np.int8:
+            f = np.ascontiguousarray(flags)
+            assert f.shape == self.state_shape[:3]
+            self._ck(self.L.dnslbm_set_flags_periodic(self.h, f.ctypes.data_as(ctypes.POINTER(ctypes.c_int8))))
+        else:
+            f = np.ascontiguousarray(flags, np.int32)
+            x, y, z = self.shape
+            assert f.shape == (x + 1, y + 1, z + 2)
+            self._ck(self.L.dnslbm_set_flags(self.h, f.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+
+    def init_rest(self):
+        self._ck(self.L.dnslbm_init_rest(self.h))
+
+    def load_state(self, state):
+        s = np.ascontiguousarray(state, np.float64)
+        assert s.shape == self.state_shape, (s.shape, self.state_shape)
+        self._ck(self.L.dnslbm_load_state(self.h, _dp(s)))
+
+    def store_state(self, out=None):
+        if out is None:
+            out = np.empty(self.state_shape, np.float64)
+        self._ck(self.L.dnslbm_store_state(self.h, _dp(out)))
+        return out
+
+    def step(self, n=1):
+        self._ck(self.L.dnslbm_step(self.h, n))
+
+    def step_timed(self, n):
+        t, e, o = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._ck(self.L.dnslbm_step_timed(self.h, n, ctypes.byref(t), ctypes.byref(e), ctypes.byref(o)))
+        return t.value, e.value, o.value
+
+    @property
+    def steps_done(self):
+        return self.L.dnslbm_steps_done(self.h)
+
+    def logs(self, first=0, count=None):
+        if count is None:
+            count = self.steps_done - first
+        out = np.zeros((count, 9), np.float64)
+        self._ck(self.L.dnslbm_logs(self.h, first, count, _dp(out)))
+        return out
+
+    def force(self):
+        v = ctypes.c_double()
+        self._ck(self.L.dnslbm_get_force(self.h, ctypes.byref(v)))
+        return v.value
+
+    def statistics(self):
+        zd = self.shape[2] + 2
+        out = np.zeros(9 * zd)
+        self._ck(self.L.dnslbm_statistics(self.h, _dp(out)))
+        return out.reshape(9, zd)
+
+    def moments(self):
+        x, y, z = self.shape
+        vel = np.zeros((x, y, z + 2, 3))
+        den = np.zeros((x, y, z + 2))
+        self._ck(self.L.dnslbm_moments(self.h, _dp(vel), _dp(den)))
+        return vel, den
+
+    @property
+    def bytes_per_cell(self):
+        return self.L.dnslbm_bytes_per_cell(self.h)
+
+    def sync(self):
+        self._ck(self.L.dnslbm_sync(self.h))
+
+
+class PinnedArray:
+    """A numpy view of page-locked host memory from dnslbm_host_alloc."""
+
+    def __init__(self, shape, dtype=np.float64):
+        self.L = lib()
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.ptr = self.L.dnslbm_host_alloc(n)
+        if not self.ptr:
+            raise MemoryError(f"dnslbm_host_alloc({n}) failed")
+        buf = (ctypes.c_char * n).from_address(self.ptr)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            self.L.dnslbm_host_free(self.ptr)
+            self.ptr = None
+
+    __del__ = free

@@ -1,0 +1,151 @@
+/*
+ * dnslbm -- B200 (sm_100a) D3Q19 BGK channel-flow time step behind a C ABI.
+ *
+ * Drop-in for the time step of the DNS solver (DNS-solver/src): the state
+ * lives in GPU memory for the whole run; the host keeps the reference's
+ * parameter deck, wall-flag semantics and file formats.  Every function
+ * returns an int status (DNSLBM_OK = 0) and never aborts; the message of the
+ * last failure is available from dnslbm_last_error().
+ *
+ * Axes and sizes follow the reference: x = i streamwise (periodic),
+ * y = j spanwise (periodic), z = k wall-normal; xdv, ydv, zdv count fluid
+ * cells (walls excluded, definitions.h:32-34); zd = zdv + 2 includes the two
+ * wall planes k = 0 and k = zd - 1.
+ *
+ * Host arrays use the reference's own layouts:
+ *   state  double [xdv][ydv][zd][19]   the lbf/ftemp layout without ghosts
+ *                                      (dns-const-q-xycut.c:405-416)
+ *   flags  int    [xdv+1][ydv+1][zd]   the reference's V.s with ghost planes
+ *                                      (solid_init.c:3-8: 0 fluid, 1 periodic,
+ *                                      -1 no-slip, -2 slip)
+ *   vel    double [xdv][ydv][zd][3], den double [xdv][ydv][zd] (vel_print.c)
+ *   stats  double [9][zd]  (statistics.c:139-147 file order)
+ *
+ * Threading: one host thread per context; each context owns one CUDA stream.
+ */
+#ifndef DNSLBM_H
+#define DNSLBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DNSLBM_OK 0
+#define DNSLBM_ERR_ARG 1      /* bad deck or argument                          */
+#define DNSLBM_ERR_CUDA 2     /* a CUDA call failed                            */
+#define DNSLBM_ERR_NAN 3      /* NaN wall shear stress (the reference aborts,  */
+                              /* wshearstr.c:126-130)                          */
+#define DNSLBM_ERR_TIMEOUT 4  /* a bounded device-side wait ran out            */
+#define DNSLBM_ERR_NOMEM 5    /* device allocation failed                      */
+#define DNSLBM_ERR_IO 6       /* file read/write failed                        */
+#define DNSLBM_ERR_STATE 7    /* call out of order (e.g. step before a state)  */
+
+/* storage precision of the populations */
+#define DNSLBM_F64 64         /* plain FP64, the reference's arithmetic order  */
+#define DNSLBM_F32 32         /* FP32 deviations f - w, FP32 collision         */
+#define DNSLBM_F16 16         /* FP16 deviations (scaled by 2^15), FP32 collision */
+
+/* body-force mode */
+#define DNSLBM_FORCE_CONST_Q 0 /* V.force = rho_mean*ub - jx_mean every step (encalc.c:121) */
+#define DNSLBM_FORCE_CONST_G 1 /* fixed body force gx                              */
+
+/* wall rule for solids inside the flow */
+#define DNSLBM_BC_REFERENCE 0 /* exactly xcomputations.c:359-400              */
+#define DNSLBM_BC_GENERAL 1   /* + halfway bounce-back on any no-slip link    */
+
+/* per-step log record: state at the start of each step, in this order */
+#define DNSLBM_LOG_FORCE 0    /* force used by the step (V.force)               */
+#define DNSLBM_LOG_RHO 1      /* mean density V.rho (encalc.c:62,79)            */
+#define DNSLBM_LOG_ENERGY 2   /* K (encalc.c:106-114) -> energy.txt             */
+#define DNSLBM_LOG_FLOWRATE 3 /* U*(ydv*zdv) (encalc.c:132) -> flowrate.txt     */
+#define DNSLBM_LOG_MASSRATE 4 /* mean jx*(ydv*zdv) (encalc.c:136) -> massrate.txt */
+#define DNSLBM_LOG_STUP 5     /* wshearstr.c:250-269 -> str-up.txt              */
+#define DNSLBM_LOG_STDOWN 6   /* wshearstr.c:203-216 -> str-do.txt              */
+#define DNSLBM_LOG_STRESS 7   /* wshearstr.c:271 -> w-str.txt                   */
+#define DNSLBM_LOG_PGRAD 8    /* wshearstr.c:265-267 -> p-grad.txt              */
+#define DNSLBM_LOG_N 9
+
+/* The parameter deck.  Replaces the compile-time #defines of
+ * definitions.h:30-59 (Rebs, ub, zdv, ydv, xdv) and the derived omega of
+ * dns-const-q-xycut.c:216-217, read at run time. */
+typedef struct dnslbm_deck {
+    int xdv, ydv, zdv;  /* fluid cells (xdv, ydv >= 2; zdv >= 3)                 */
+    double omega;       /* relaxation rate 1/tau (the reference's `tau` variable) */
+    double ubulk;       /* target bulk velocity (constant-Q)                     */
+    double gx;          /* body force (constant-g)                               */
+    int force_mode;     /* DNSLBM_FORCE_*                                        */
+    int precision;      /* DNSLBM_F64 | DNSLBM_F32 | DNSLBM_F16                  */
+    int bc_mode;        /* DNSLBM_BC_*                                           */
+    int log_capacity;   /* per-step records kept on the device (0 -> 4096)       */
+    int device;         /* CUDA device ordinal                                   */
+} dnslbm_deck;
+
+typedef struct dnslbm_ctx dnslbm_ctx;
+
+/* Allocate a device context for the deck.  Replaces the calloc block of
+ * dns-const-q-xycut.c:239-356 and the halo request set-up of :363-376 (the
+ * halo exchange is an in-kernel periodic wrap here).  Flags default to
+ * solid_init (smooth no-slip walls). */
+int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out);
+void dnslbm_destroy(dnslbm_ctx *ctx);
+/* message of the last failure of this context (ctx NULL: of the last failed
+ * dnslbm_create on this thread) */
+const char *dnslbm_last_error(const dnslbm_ctx *ctx);
+
+/* Wall flags in the reference's V.s layout with ghost planes.  Replaces
+ * solid_init.c:10-46, slip_ridges_init.c:3-43 and slip_posts_init.c:3-74 as
+ * inputs to the step; the ghost planes are ignored (the grid is periodic). */
+int dnslbm_set_flags(dnslbm_ctx *ctx, const int *s);
+/* The same on the ghost-free periodic grid: int8 [xdv][ydv][zd]. */
+int dnslbm_set_flags_periodic(dnslbm_ctx *ctx, const int8_t *flags);
+
+/* Initial state: rest, f = w (init.c:6-19). */
+int dnslbm_init_rest(dnslbm_ctx *ctx);
+/* Load / store the state in the lbf ftemp layout (dns-const-q-xycut.c:405-416
+ * read, :494-497 write).  Wall-plane entries are ignored on load and written
+ * as zeros on store.  Loading resets the step counter. */
+int dnslbm_load_state(dnslbm_ctx *ctx, const double *state);
+int dnslbm_store_state(dnslbm_ctx *ctx, double *state);
+
+/* Advance nsteps time steps on the device.  Each step is the reference's loop
+ * body (dns-const-q-xycut.c:487-518): the encalc/wshearstr reductions of the
+ * state (logged), then collide + stream + wall rules + periodic wrap
+ * (xcomputations.c:5-562).  Returns DNSLBM_ERR_NAN if any step saw a NaN wall
+ * stress. */
+int dnslbm_step(dnslbm_ctx *ctx, long nsteps);
+/* Steps done since the last load/init. */
+long dnslbm_steps_done(const dnslbm_ctx *ctx);
+/* Copy the log records of steps [first, first+count) (count*DNSLBM_LOG_N
+ * doubles); only the last log_capacity steps are kept. */
+int dnslbm_logs(dnslbm_ctx *ctx, long first, long count, double *out);
+/* Force the next step will use (V.force). */
+int dnslbm_get_force(dnslbm_ctx *ctx, double *force);
+
+/* statistics.c:3-183 of the current state: out[9*zd]. */
+int dnslbm_statistics(dnslbm_ctx *ctx, double *out);
+/* vel_print.c:65-99 of the current state (either pointer may be NULL). */
+int dnslbm_moments(dnslbm_ctx *ctx, double *vel, double *den);
+
+/* Timing support for benchmarks: advance nsteps like dnslbm_step and return
+ * CUDA-event times on the context's stream: total, and the summed device
+ * time of the two step kernels (even / odd parity launches). */
+int dnslbm_step_timed(dnslbm_ctx *ctx, long nsteps, double *ms_total, double *ms_even, double *ms_odd);
+/* Populations bytes moved per fluid cell per step (2*19*storage bytes). */
+double dnslbm_bytes_per_cell(const dnslbm_ctx *ctx);
+/* Block until all work of the context is done. */
+int dnslbm_sync(dnslbm_ctx *ctx);
+
+/* Page-locked host memory for state buffers (faster load/store); NULL on
+ * failure.  Replaces nothing in the reference (its arrays are calloc'ed,
+ * dns-const-q-xycut.c:248-262). */
+void *dnslbm_host_alloc(size_t bytes);
+void dnslbm_host_free(void *ptr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,195 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the oracle.
+
+Tolerances (written here):
+  * FP64, constant g: bit-identical populations to the reference (goldens)
+    and to the oracle, for every texture, grid and step count (either AA
+    parity).  Logs: force exact; reductions within 1e-12 relative (only the
+    summation order differs from the reference's sequential sums).
+  * FP64, constant Q: the force of each step comes from a differently ordered
+    FP64 sum, so populations agree to <= 1e-12 relative.
+  * FP32 / FP16 storage: errors against the FP64 oracle are measured and
+    bounded in test_lowp_precision.py.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import dnslbm
+import inputs
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def gpu_run(s0, flags, omega, steps, gx=0.0, ubulk=0.0, const_g=True, precision=64, chunks=None):
+    nx, ny, zd, _ = s0.shape
+    ch = dnslbm.Channel(nx, ny, zd - 2, omega, ubulk=ubulk, gx=gx,
+                        force_mode=dnslbm.CONST_G if const_g else dnslbm.CONST_Q, precision=precision)
+    ch.set_flags(flags)
+    ch.load_state(s0)
+    for n in (chunks or [steps]):
+        ch.step(n)
+    return ch
+
+
+def ref_flags(oracle, tex, nx, ny, nz):
+    return oracle.flags(tex, nx, ny, nz)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_f64_matches_reference_golden(oracle_mod, path):
+    g = np.load(path)
+    nx, ny, nz = (int(v) for v in g["dims"])
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, int(g["seed"]))
+    steps, cg = int(g["steps"]), bool(g["const_g"])
+    fl = ref_flags(oracle_mod, str(g["texture"]), nx, ny, nz)
+    ch = gpu_run(s0, fl, float(g["omega"]), steps, gx=float(g["gx"]), ubulk=float(g["ubulk"]), const_g=cg,
+                 chunks=[steps - 1, 1])
+    st = ch.store_state()
+    logs = ch.logs()
+    if cg:
+        np.testing.assert_array_equal(st, g["state"])
+        np.testing.assert_array_equal(logs[:, 0], g["force"])
+    else:
+        np.testing.assert_allclose(st, g["state"], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(logs[:, 0], g["force"], rtol=1e-9, atol=1e-15)
+    np.testing.assert_allclose(logs[:, 1], g["rho"], rtol=1e-13)
+    # text logs are printed with 12-14 decimals by the reference
+    np.testing.assert_allclose(logs[:, 2:], g["logs"], rtol=0, atol=6e-13)
+
+
+@pytest.mark.parametrize("steps", [1, 2, 5, 8])
+@pytest.mark.parametrize("tex", ["smooth", "ridges", "posts"])
+def test_f64_bitexact_any_parity(oracle_mod, tex, steps):
+    nx, ny, nz = 16, 12, 7
+    fl = ref_flags(oracle_mod, tex, nx, ny, nz)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 7)
+    ref = s0.copy()
+    rlogs = oracle_mod.run(ref, fl, 1.85, gx=3e-5, const_g=True, nsteps=steps)
+    ch = gpu_run(s0, fl, 1.85, steps, gx=3e-5)
+    np.testing.assert_array_equal(ch.store_state(), ref)
+    logs = ch.logs()
+    np.testing.assert_array_equal(logs[:, 0], rlogs[:, 0])
+    np.testing.assert_allclose(logs[:, 1:], rlogs[:, 1:], rtol=1e-11, atol=1e-15)
+
+
+@pytest.mark.parametrize("dims", [(9, 5, 3), (13, 7, 4), (33, 17, 9), (130, 3, 5)])
+def test_f64_bitexact_ragged_grids_transverse(oracle_mod, dims):
+    """Odd sizes, rows narrower and wider than a block, transverse grooves."""
+    nx, ny, nz = dims
+    fl = inputs.flags_transverse(nx, ny, nz, 2, 3)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.06, 0.1, 3)
+    ref = s0.copy()
+    oracle_mod.run(ref, fl, 1.7, gx=1e-5, const_g=True, nsteps=11)
+    ch = gpu_run(s0, fl, 1.7, 11, gx=1e-5)
+    np.testing.assert_array_equal(ch.store_state(), ref)
+
+
+@pytest.mark.parametrize("tex", ["smooth", "posts"])
+def test_f64_constant_q(oracle_mod, tex):
+    nx, ny, nz = 24, 16, 10
+    fl = ref_flags(oracle_mod, tex, nx, ny, nz)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 5)
+    ref = s0.copy()
+    rlogs = oracle_mod.run(ref, fl, 1.6, ubulk=0.07, const_g=False, nsteps=20)
+    ch = gpu_run(s0, fl, 1.6, 20, ubulk=0.07, const_g=False)
+    st = ch.store_state()
+    np.testing.assert_allclose(st, ref, rtol=1e-12, atol=0)
+    logs = ch.logs()
+    np.testing.assert_allclose(logs[:, 0], rlogs[:, 0], rtol=1e-9, atol=1e-16)
+    np.testing.assert_allclose(ch.force(), oracle_mod.encalc(ref, 0.07)[0], rtol=1e-9, atol=1e-16)
+
+
+@pytest.mark.parametrize("steps", [4, 5])
+def test_statistics_and_moments(oracle_mod, steps):
+    nx, ny, nz = 20, 12, 8
+    fl = inputs.flags_longitudinal(nx, ny, nz, 2, 2)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 9)
+    ref = s0.copy()
+    oracle_mod.run(ref, fl, 1.5, gx=2e-5, const_g=True, nsteps=steps)
+    ch = gpu_run(s0, fl, 1.5, steps, gx=2e-5)
+    vel, den = ch.moments()
+    rvel, rden = oracle_mod.moments(ref)
+    np.testing.assert_array_equal(vel, rvel)
+    np.testing.assert_array_equal(den, rden)
+    np.testing.assert_allclose(ch.statistics(), oracle_mod.statistics(ref), rtol=1e-11, atol=1e-15)
+
+
+def test_laminar64_1000_steps_bitexact(oracle_mod):
+    """The first workload: 64 x 66 x 32, tau 0.52, g 1e-6, 1000 steps."""
+    wl = inputs.workload("laminar64")
+    s0 = inputs.make_state(wl, seed=0)
+    fl = inputs.make_flags(wl)
+    ref = s0.copy()
+    rlogs = oracle_mod.run(ref, fl, wl.omega, gx=wl.gx, const_g=True, nsteps=wl.steps)
+    ch = gpu_run(s0, fl, wl.omega, wl.steps, gx=wl.gx)
+    np.testing.assert_array_equal(ch.store_state(), ref)
+    np.testing.assert_allclose(ch.logs()[:, 1:], rlogs[:, 1:], rtol=1e-10, atol=1e-15)
+
+
+def test_rest_start_matches_reference_init(oracle_mod):
+    """init.c rest state, constant Q: the flow accelerates from rest."""
+    nx, ny, nz = 12, 8, 6
+    ch = dnslbm.Channel(nx, ny, nz, 1.4, ubulk=0.05, force_mode=dnslbm.CONST_Q)
+    ch.init_rest()
+    ch.step(9)
+    s0 = np.zeros((nx, ny, nz + 2, 19))
+    s0[:, :, 1:nz + 1] = inputs.W
+    ref = s0.copy()
+    oracle_mod.run(ref, oracle_mod.flags("smooth", nx, ny, nz), 1.4, ubulk=0.05, const_g=False, nsteps=9)
+    np.testing.assert_allclose(ch.store_state(), ref, rtol=1e-12, atol=1e-18)
+
+
+def test_load_store_roundtrip_and_wall_zeros():
+    nx, ny, nz = 10, 6, 5
+    s0 = inputs.laminar_state(nx, ny, nz, 0.05, 0.1, 1)
+    ch = dnslbm.Channel(nx, ny, nz, 1.2)
+    ch.load_state(s0)
+    out = ch.store_state()
+    np.testing.assert_array_equal(out, s0)
+    assert not out[:, :, 0].any() and not out[:, :, -1].any()
+
+
+def test_nan_is_reported_not_aborted():
+    nx, ny, nz = 8, 6, 5
+    s0 = inputs.laminar_state(nx, ny, nz, 0.05, 0.1, 1)
+    s0[3, 2, 1, 4] = np.nan  # a NaN in the wall-adjacent plane reaches the wall stress
+    ch = dnslbm.Channel(nx, ny, nz, 1.2, gx=1e-6)
+    ch.load_state(s0)
+    with pytest.raises(dnslbm.DnsLbmError) as e:
+        ch.step(3)
+    assert e.value.code == dnslbm.ERR_NAN
+    # the context stays usable: a clean state steps again
+    ch.load_state(inputs.laminar_state(nx, ny, nz, 0.05, 0.1, 2))
+    ch.step(2)
+
+
+def test_flag_validation():
+    nx, ny, nz = 8, 6, 5
+    ch = dnslbm.Channel(nx, ny, nz, 1.2)
+    fl = inputs.flags_smooth(nx, ny, nz)
+    fl[2, 2, 3] = -1  # a solid inside the flow
+    with pytest.raises(dnslbm.DnsLbmError) as e:
+        ch.set_flags(fl)
+    assert e.value.code == dnslbm.ERR_ARG
+    fl = inputs.flags_smooth(nx, ny, nz)
+    fl[1, 1, 0] = 0  # a fluid cell in the wall plane
+    with pytest.raises(dnslbm.DnsLbmError):
+        ch.set_flags(fl)
+
+
+def test_reference_ghost_flag_array(oracle_mod):
+    """dnslbm_set_flags takes the reference's V.s array with ghost planes."""
+    nx, ny, nz = 12, 8, 6
+    fl = oracle_mod.flags("posts", nx, ny, nz)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 4)
+    ch = dnslbm.Channel(nx, ny, nz, 1.3, gx=1e-5)
+    ch.set_flags(oracle_mod.ghost_flags(fl))
+    ch.load_state(s0)
+    ch.step(6)
+    ref = s0.copy()
+    oracle_mod.run(ref, fl, 1.3, gx=1e-5, const_g=True, nsteps=6)
+    np.testing.assert_array_equal(ch.store_state(), ref)

@@ -1,0 +1,62 @@
+"""FP32 / FP16 deviation storage against the FP64 oracle.
+
+Each result states its error against the FP64 oracle (the CPU restatement,
+which the FP64 GPU kernel matches bit for bit).  Bounds asserted here:
+  FP32: populations within 2e-7 absolute after 200 laminar steps; the mean
+        velocity profile within 1e-5 relative.
+  FP16: populations within 2e-4 absolute; the mean velocity profile within
+        0.5 % (the north-star bound for the long-run profile).
+"""
+import numpy as np
+import pytest
+
+import dnslbm
+import inputs
+
+pytestmark = pytest.mark.gpu
+
+BOUNDS = {32: (2e-7, 1e-5), 16: (2e-4, 5e-3)}
+
+
+def run(prec, s0, fl, omega, gx, steps):
+    nx, ny, zd, _ = s0.shape
+    with dnslbm.Channel(nx, ny, zd - 2, omega, gx=gx, force_mode=dnslbm.CONST_G, precision=prec) as ch:
+        ch.set_flags(fl)
+        ch.load_state(s0)
+        ch.step(steps)
+        return ch.store_state(), ch.statistics(), ch.logs()
+
+
+@pytest.mark.parametrize("prec", [32, 16])
+def test_laminar_against_f64_oracle(oracle_mod, prec):
+    nx, ny, nz = 32, 16, 30
+    s0 = inputs.laminar_state(nx, ny, nz, 0.05, 0.01, 0)
+    fl = inputs.flags_smooth(nx, ny, nz)
+    ref = s0.copy()
+    oracle_mod.run(ref, fl, 1 / 0.52, gx=1e-6, const_g=True, nsteps=200)
+    st, stats, logs = run(prec, s0, fl, 1 / 0.52, 1e-6, 200)
+    pop_err = np.abs(st - ref).max()
+    um_ref = oracle_mod.statistics(ref)[0, 1:-1]
+    prof_err = np.abs(stats[0, 1:-1] - um_ref).max() / np.abs(um_ref).max()
+    print(f"FP{prec}: max |f - f_oracle| = {pop_err:.3e}, mean-u profile rel err = {prof_err:.3e}")
+    assert pop_err < BOUNDS[prec][0]
+    assert prof_err < BOUNDS[prec][1]
+
+
+@pytest.mark.parametrize("prec", [32, 16])
+def test_grooved_turbulent_like_against_f64_oracle(oracle_mod, prec):
+    nx, ny, nz = 48, 32, 24
+    s0 = inputs.turbulent_state(nx, ny, nz, 0.08, 0.1, 2)
+    fl = inputs.flags_longitudinal(nx, ny, nz, 4, 4)
+    ref = s0.copy()
+    oracle_mod.run(ref, fl, 1.9, gx=2e-6, const_g=True, nsteps=50)
+    st, stats, logs = run(prec, s0, fl, 1.9, 2e-6, 50)
+    vref, _ = oracle_mod.moments(ref)
+    vel = np.empty_like(vref)
+    with dnslbm.Channel(nx, ny, nz, 1.9, gx=2e-6, precision=64) as ch:
+        ch.set_flags(fl)
+        ch.load_state(st)
+        vel, _ = ch.moments()
+    err = np.abs(vel - vref).max() / 0.08
+    print(f"FP{prec}: max cell velocity error / U_b after 50 steps = {err:.3e}")
+    assert err < (1e-5 if prec == 32 else 5e-3)
