@@ -1,0 +1,337 @@
+/*
+ * run-dns: the channel-flow DNS driver on one B200, through the dnslbm C ABI.
+ *
+ * Mirrors the reference's main program (DNS-solver/src/dns-const-q-xycut.c)
+ * with its deck, start modes and output files; the time step itself runs on
+ * the GPU.  Usage, as the reference's (README "Usage"):
+ *
+ *     run-dns -s|-p [deck-file] [NAME=value ...]
+ *
+ *   -s  fresh start from rest (init.c), flags from the deck's texture
+ *   -p  restart from lbf.TSTR (ftemp then f, [xdv][ydv][zd][19] doubles)
+ *       and force.TSTR (one double), dns-const-q-xycut.c:399-454
+ *
+ * Deck (file lines "NAME value", or NAME=value arguments): the reference's
+ * compile-time names Rebs ub zdv ydv xdv TSTR TEND CFL ITER (definitions.h:
+ * 30-52) and RSLIP / PSLIP (set to 1 to select those textures with the
+ * reference's constants), plus
+ *   TEXTURE smooth|ridges|transverse|posts   GAP WIDTH   PGX PWX PGY PWY
+ *   PRECISION 64|32|16   FORCE q|g   GX   DEVICE   OMEGA (overrides Rebs)
+ *
+ * Files written (formats of the reference):
+ *   energy.txt flowrate.txt massrate.txt   encalc.c:125-138, every step
+ *   str-up.txt str-do.txt w-str.txt p-grad.txt   wshearstr.c:278-300
+ *   lbf.NNNN force.NNNN   every 10*utime steps, dns-const-q-xycut.c:491-513
+ *   vel.NNNN den.NNNN     every utime steps, vel_print.c
+ *   turb-fld.000.TTT uavg-temp.dat   every utime steps, statistics.c:135-165
+ *   report.code           dns-const-q-xycut.c:522-540
+ * The lbf file's second half (the reference's f array, whose values the next
+ * step overwrites before reading) holds the state again.
+ */
+#include <errno.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "../../include/dnslbm.h"
+#include "textures.h"
+
+typedef struct {
+    double Rebs, ub, CFL, GX, OMEGA;
+    int zdv, ydv, xdv, TSTR, TEND, ITER, RSLIP, PSLIP;
+    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY;
+    char TEXTURE[32], FORCE[8];
+} Deck;
+
+static void deck_defaults(Deck *d)
+{
+    /* the reference's shipped deck, definitions.h:30-37 */
+    memset(d, 0, sizeof *d);
+    d->Rebs = 100.0;
+    d->ub = 0.1;
+    d->zdv = 25;
+    d->ydv = 8;
+    d->xdv = 16;
+    d->TSTR = 420;
+    d->TEND = 440;
+    d->CFL = 0.1;
+    d->ITER = -1;
+    d->PRECISION = 64;
+    d->GAP = 2;
+    d->WIDTH = 2;
+    d->PGX = 2;
+    d->PWX = 2;
+    d->PGY = 2;
+    d->PWY = 2;
+    strcpy(d->TEXTURE, "smooth");
+    strcpy(d->FORCE, "q");
+}
+
+static int deck_set(Deck *d, const char *k, const char *v)
+{
+#define DBL(N) if (!strcmp(k, #N)) { d->N = atof(v); return 0; }
+#define INT(N) if (!strcmp(k, #N)) { d->N = atoi(v); return 0; }
+#define STR(N) if (!strcmp(k, #N)) { snprintf(d->N, sizeof d->N, "%s", v); return 0; }
+    DBL(Rebs) DBL(ub) DBL(CFL) DBL(GX) DBL(OMEGA)
+    INT(zdv) INT(ydv) INT(xdv) INT(TSTR) INT(TEND) INT(ITER) INT(RSLIP) INT(PSLIP)
+    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY)
+    STR(TEXTURE) STR(FORCE)
+#undef DBL
+#undef INT
+#undef STR
+    fprintf(stderr, "run-dns: unknown deck entry %s\n", k);
+    return -1;
+}
+
+static int deck_read(Deck *d, const char *path)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    char line[256], k[64], v[128];
+    while (fgets(line, sizeof line, f)) {
+        char *h = strchr(line, '#');
+        if (h) *h = 0;
+        for (char *p = line; *p; p++)
+            if (*p == '=') *p = ' ';
+        if (sscanf(line, "%63s %127s", k, v) == 2 && deck_set(d, k, v)) {
+            fclose(f);
+            return -2;
+        }
+    }
+    fclose(f);
+    return 0;
+}
+
+static int die(dnslbm_ctx *c, int rc, const char *what)
+{
+    fprintf(stderr, "run-dns: %s failed (%d): %s\n", what, rc, dnslbm_last_error(c));
+    return 1;
+}
+
+static void append(const char *fn, const char *fmt, double t, double v)
+{
+    FILE *f = fopen(fn, "a");
+    if (!f) return;
+    fprintf(f, fmt, t, v);
+    fclose(f);
+}
+
+static int write_file(const char *fn, const void *p, size_t bytes, size_t copies)
+{
+    FILE *f = fopen(fn, "wb");
+    if (!f) return -1;
+    for (size_t i = 0; i < copies; i++)
+        if (fwrite(p, 1, bytes, f) != bytes) {
+            fclose(f);
+            return -1;
+        }
+    return fclose(f);
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 2 || (strcmp(argv[1], "-s") && strcmp(argv[1], "-p"))) {
+        fprintf(stderr, "usage: run-dns -s|-p [deck-file] [NAME=value ...]\n");
+        return 2;
+    }
+    Deck D;
+    deck_defaults(&D);
+    int a = 2;
+    if (argc > 2 && !strchr(argv[2], '=')) {
+        if (deck_read(&D, argv[2])) {
+            fprintf(stderr, "run-dns: cannot read deck %s\n", argv[2]);
+            return 2;
+        }
+        a = 3;
+    }
+    for (; a < argc; a++) {
+        char k[64];
+        const char *eq = strchr(argv[a], '=');
+        if (!eq || eq - argv[a] >= (long)sizeof k) return 2;
+        memcpy(k, argv[a], eq - argv[a]);
+        k[eq - argv[a]] = 0;
+        if (deck_set(&D, k, eq + 1)) return 2;
+    }
+    if (D.RSLIP) strcpy(D.TEXTURE, "ridges");
+    if (D.PSLIP) strcpy(D.TEXTURE, "posts");
+
+    /* derived parameters, dns-const-q-xycut.c:55,203-237 */
+    const int zd = D.zdv + 2;
+    double utime_d = 0.5 * (zd - 2.) / D.CFL;
+    const double dt = 1. / utime_d;
+    const long utime = (long)utime_d;
+    double tau = (3. / D.Rebs) * D.ub * (zd - 2.) + 0.5;
+    double omega = D.OMEGA > 0 ? D.OMEGA : 1. / tau;
+    long up = (long)(D.TEND - D.TSTR) * utime;
+    if (D.ITER >= 0) up = D.ITER;
+    if (utime < 1) {
+        fprintf(stderr, "run-dns: CFL gives less than one step per time unit\n");
+        return 2;
+    }
+
+    dnslbm_deck dk = {D.xdv, D.ydv, D.zdv, omega, D.ub, D.GX,
+                      D.FORCE[0] == 'g' ? DNSLBM_FORCE_CONST_G : DNSLBM_FORCE_CONST_Q,
+                      D.PRECISION, DNSLBM_BC_REFERENCE, 0, D.DEVICE};
+    dnslbm_ctx *c = NULL;
+    int rc = dnslbm_create(&dk, &c);
+    if (rc) return die(NULL, rc, "dnslbm_create");
+
+    const size_t nflag = (size_t)D.xdv * D.ydv * zd;
+    int8_t *flags = malloc(nflag);
+    const size_t ncol = (size_t)D.xdv * D.ydv, state_n = ncol * zd * 19;
+    double *state = malloc(state_n * sizeof(double));
+    if (!flags || !state) {
+        fprintf(stderr, "run-dns: host allocation failed: %s\n", strerror(errno));
+        return 1;
+    }
+    if (!strcmp(D.TEXTURE, "smooth")) tex_smooth(D.xdv, D.ydv, D.zdv, flags);
+    else if (!strcmp(D.TEXTURE, "ridges")) tex_longitudinal(D.xdv, D.ydv, D.zdv, D.GAP, D.WIDTH, flags);
+    else if (!strcmp(D.TEXTURE, "transverse")) tex_transverse(D.xdv, D.ydv, D.zdv, D.GAP, D.WIDTH, flags);
+    else if (!strcmp(D.TEXTURE, "posts")) tex_posts(D.xdv, D.ydv, D.zdv, D.PGX, D.PWX, D.PGY, D.PWY, flags);
+    else {
+        fprintf(stderr, "run-dns: unknown texture %s\n", D.TEXTURE);
+        return 2;
+    }
+    if ((rc = dnslbm_set_flags_periodic(c, flags))) return die(c, rc, "dnslbm_set_flags_periodic");
+
+    char fn[64];
+    int TM;
+    if (argv[1][1] == 's') {
+        TM = D.TSTR;
+        if ((rc = dnslbm_init_rest(c))) return die(c, rc, "dnslbm_init_rest");
+    } else {
+        fprintf(stderr, "TRYING TO READ DATA FROM FILES\n");
+        snprintf(fn, sizeof fn, "lbf.%.4d", D.TSTR);
+        FILE *f = fopen(fn, "rb");
+        if (!f || fread(state, sizeof(double), state_n, f) != state_n) {
+            fprintf(stderr, "run-dns: cannot read %s (need %zu doubles of ftemp)\n", fn, state_n);
+            return 1;
+        }
+        fclose(f);
+        snprintf(fn, sizeof fn, "force.%.4d", D.TSTR);
+        f = fopen(fn, "rb");
+        double force = 0.;
+        if (f) {
+            if (fread(&force, sizeof force, 1, f) != 1) force = 0.;
+            fclose(f);
+        }
+        if ((rc = dnslbm_load_state(c, state))) return die(c, rc, "dnslbm_load_state");
+        TM = D.TSTR;
+        fprintf(stderr, "END OF READING DATA FROM FILES\nSTARTING FROM %d\n", TM);
+    }
+
+    double *vel = malloc(ncol * zd * 3 * sizeof(double)), *den = malloc(ncol * zd * sizeof(double));
+    double *stats = malloc(9 * zd * sizeof(double));
+    const long cap = 4096;
+    double *logs = malloc(cap * DNSLBM_LOG_N * sizeof(double));
+    if (!vel || !den || !stats || !logs) {
+        fprintf(stderr, "run-dns: host allocation failed\n");
+        return 1;
+    }
+
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    long ss = 0;
+    int nan_stop = 0;
+    while (ss < up + 1 && !nan_stop) {
+        if (!(ss % utime)) {
+            const long label = TM + ss / utime;
+            if (!(ss % (10 * utime))) {
+                if ((rc = dnslbm_store_state(c, state))) return die(c, rc, "dnslbm_store_state");
+                snprintf(fn, sizeof fn, "lbf.%.4ld", label);
+                if (write_file(fn, state, state_n * sizeof(double), 2)) return die(c, DNSLBM_ERR_IO, fn);
+                double force;
+                if ((rc = dnslbm_get_force(c, &force))) return die(c, rc, "dnslbm_get_force");
+                snprintf(fn, sizeof fn, "force.%.4ld", label);
+                if (write_file(fn, &force, sizeof force, 1)) return die(c, DNSLBM_ERR_IO, fn);
+            }
+            if ((rc = dnslbm_moments(c, vel, den))) return die(c, rc, "dnslbm_moments");
+            snprintf(fn, sizeof fn, "vel.%.4d", (int)label);
+            if (write_file(fn, vel, ncol * zd * 3 * sizeof(double), 1)) return die(c, DNSLBM_ERR_IO, fn);
+            snprintf(fn, sizeof fn, "den.%.4d", (int)label);
+            if (write_file(fn, den, ncol * zd * sizeof(double), 1)) return die(c, DNSLBM_ERR_IO, fn);
+            if ((rc = dnslbm_statistics(c, stats))) return die(c, rc, "dnslbm_statistics");
+            snprintf(fn, sizeof fn, "turb-fld.%.3d.%.3ld", 0, label);
+            if (write_file(fn, stats, 9 * zd * sizeof(double), 1)) return die(c, DNSLBM_ERR_IO, fn);
+            FILE *u = fopen("uavg-temp.dat", "w");
+            if (u) {
+                for (int k = 0; k < zd; k++) {
+                    double z = k == 0 ? 0. : (k == zd - 1 ? zd - 2. : k - 0.5);
+                    fprintf(u, "%.12f %.12f\n", z / (zd - 2.), stats[k]);
+                }
+                fclose(u);
+            }
+        }
+        /* steps up to the next output event, in one device batch */
+        long n = utime - ss % utime;
+        if (n > up + 1 - ss) n = up + 1 - ss;
+        if (n > cap) n = cap;
+        rc = dnslbm_step(c, n);
+        long have = n;
+        if (rc == DNSLBM_ERR_NAN) {
+            /* logs up to the failing step, then stop as the reference's abort() */
+            long first_bad = n;
+            double *tmp = logs;
+            dnslbm_logs(c, dnslbm_steps_done(c) - n, n, tmp);
+            for (long i = 0; i < n; i++)
+                if (tmp[i * DNSLBM_LOG_N + DNSLBM_LOG_STRESS] != tmp[i * DNSLBM_LOG_N + DNSLBM_LOG_STRESS]) {
+                    first_bad = i;
+                    break;
+                }
+            have = first_bad;
+            nan_stop = 1;
+        } else if (rc) {
+            return die(c, rc, "dnslbm_step");
+        } else if ((rc = dnslbm_logs(c, dnslbm_steps_done(c) - n, n, logs))) {
+            return die(c, rc, "dnslbm_logs");
+        }
+        for (long i = 0; i < have; i++) {
+            const double *r = logs + i * DNSLBM_LOG_N;
+            const double t = (double)TM + dt * (ss + i);
+            append("energy.txt", "%f %.14f\n", t, r[DNSLBM_LOG_ENERGY]);
+            append("flowrate.txt", "%f %.12f\n", t, r[DNSLBM_LOG_FLOWRATE]);
+            append("massrate.txt", "%f %.12f\n", t, r[DNSLBM_LOG_MASSRATE]);
+            append("str-up.txt", "%f %.12f\n", t, r[DNSLBM_LOG_STUP]);
+            append("str-do.txt", "%f %.12f\n", t, r[DNSLBM_LOG_STDOWN]);
+            append("w-str.txt", "%f %.12f\n", t, r[DNSLBM_LOG_STRESS]);
+            append("p-grad.txt", "%f %.12f\n", t, r[DNSLBM_LOG_PGRAD]);
+        }
+        if (nan_stop && have < n) {
+            /* energy/flowrate/massrate of the failing step come before the
+             * check in the reference (encalc runs before wshearstr) */
+            const double *r = logs + have * DNSLBM_LOG_N;
+            const double t = (double)TM + dt * (ss + have);
+            append("energy.txt", "%f %.14f\n", t, r[DNSLBM_LOG_ENERGY]);
+            append("flowrate.txt", "%f %.12f\n", t, r[DNSLBM_LOG_FLOWRATE]);
+            append("massrate.txt", "%f %.12f\n", t, r[DNSLBM_LOG_MASSRATE]);
+            fprintf(stderr, "Eroor: NAN, found in wall shear stress\n");
+        }
+        ss += n;
+    }
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    const double secs = (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+
+    FILE *tm = fopen("report.code", "w");
+    if (tm) {
+        fprintf(tm, "xd=%d,yd=%d,zd+2=%d,Reb=%f,tau=%f,G=%.10f,Ub=%f,CFLnumber=%f\n", D.xdv + 1, D.ydv + 1, zd,
+                D.Rebs, omega, D.GX, D.ub, D.CFL);
+        fprintf(tm, "number of processors: 1 GPU (device %d)\n", D.DEVICE);
+        fprintf(tm, "Executed File's Name: %s\n", __FILE__);
+        fprintf(tm, "Compilation Option: dnslbm fp%d\n", D.PRECISION);
+        fprintf(tm, "slip option: %s\n", D.TEXTURE);
+        fprintf(tm, "Total computational time is: %f s\n", secs);
+        fprintf(tm, "Unit non-dimensional time is: %f iterations\n", (double)utime);
+        fprintf(tm, "Starting time: %d\n", D.TSTR);
+        fprintf(tm, "Current Time is: %d\n", D.TEND);
+        fclose(tm);
+    }
+    free(flags);
+    free(state);
+    free(vel);
+    free(den);
+    free(stats);
+    free(logs);
+    dnslbm_destroy(c);
+    return nan_stop ? 1 : 0;
+}
