@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="channel180")
+    ap.add_argument("--precision", type=int, choices=[64, 32, 16], default=64,
+                    help="storage precision of the headline run (profiling other kernels)")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -237,7 +239,7 @@ def run_ours(args):
     peak, peak_src = hbm_peak()
 
     ch = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, ubulk=wl.ubulk, gx=wl.gx, force_mode=dnslbm.CONST_G,
-                        precision=64, device=dev)
+                        precision=args.precision, device=dev)
     ch.set_flags(flags)
     ch.load_state(s0)
     ch.step_timed(args.warmup)
@@ -252,20 +254,21 @@ def run_ours(args):
     value = d.world * cells * args.steps / (tmax / 1e3) / 1e6
     bpc = ch.bytes_per_cell
     # dominant kernel: the parity with the larger summed device time
+    kbase = "step_f64_kernel" if args.precision == 64 else f"step_lp_kernel<fp{args.precision}>"
     if odd >= even:
-        kname, kms, kn = "step_f64_kernel<odd>", odd, n_odd
+        kname, kms, kn = kbase + "<odd>", odd, n_odd
     else:
-        kname, kms, kn = "step_f64_kernel<even>", even, n_even
+        kname, kms, kn = kbase + "<even>", even, n_even
     launch_s = kms / kn / 1e3
     achieved = bpc * cells / launch_s / 1e9
-    traffic = ncu_traffic(f"{wl.name}:f64")
+    traffic = ncu_traffic(f"{wl.name}:f{args.precision}")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": f"{peak_src} (MEASURED_PEAKS.json)",
             "kernel": kname, "launch_ms": round(launch_s * 1e3, 4),
             "algorithmic_bytes_per_launch": bpc * cells, "bytes_per_cell": bpc}
 
     variants = {}
-    if not args.no_variants:
+    if not args.no_variants and args.precision == 64:
         ref_stats = ch.statistics()
         ref_vel, _ = ch.moments()
         done = ch.steps_done
@@ -336,13 +339,13 @@ def run_ours(args):
     if d.rank == 0:
         line = {"metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": d.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tmax / args.steps, 4),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": f"f{args.precision}",
                 "data": "synthetic (seeded turbulent-like field: laminar profile + divergence-free perturbation "
                         "of 10% of U_b)",
                 "config": {"workload": wl.name, "grid": f"{wl.nx}x{wl.nz + 2}x{wl.ny}", "cells": cells,
                            "walls": wl.texture, "force": f"constant g={wl.gx:.3e}", "omega": wl.omega,
                            "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU",
-                           "l2": "state 6.0 GB >> 126 MB L2, no flush"},
+                           "l2": f"state {cells * 19 * args.precision / 8 / 1e9:.2f} GB vs 126 MB L2, no flush"},
                 "roofline": roof, "variants": variants, "e2e": e2e, "cpu_baseline": cb,
                 "gpu_launches": args.steps, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)

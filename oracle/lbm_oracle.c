@@ -55,8 +55,9 @@ static inline void collide(double *f, double omega, double Gx)
     }
 }
 
-int orc_step(int nx, int ny, int nz, double *state, double *scratch, const int8_t *flags,
-             double omega, double force, int bc_mode)
+/* one step from `src` (collided) streamed into `dst` */
+static void orc_step_ab(int nx, int ny, int nz, const double *src, double *dst, const int8_t *flags,
+                        double omega, double force, int bc_mode)
 {
     const int zd = nz + 2;
     /* Each fluid destination slot has exactly one writer (a permutation), so
@@ -67,7 +68,7 @@ int orc_step(int nx, int ny, int nz, double *state, double *scratch, const int8_
         for (int y = 0; y < ny; y++) {
             for (int z = 1; z < zd - 1; z++) {
                 if (flags[IDX(x, y, z)] != 0) continue;
-                memcpy(f, state + IDX(x, y, z) * 19, sizeof f);
+                memcpy(f, src + IDX(x, y, z) * 19, sizeof f);
                 collide(f, omega, force);
                 /* streaming + wall rules, xcomputations.c:359-376 */
                 for (int a = 0; a < 19; a++) {
@@ -77,25 +78,48 @@ int orc_step(int nx, int ny, int nz, double *state, double *scratch, const int8_
                     int sld = flags[IDX(xt, yt, zt)];
                     int sld1 = flags[IDX(x, y, zt)];
                     if (sld > -1) {
-                        scratch[IDX(xt, yt, zt) * 19 + a] = f[a];
+                        dst[IDX(xt, yt, zt) * 19 + a] = f[a];
                     } else if (sld == -1 && sld1 == -1) {
-                        scratch[IDX(x, y, z) * 19 + OPP[a]] = f[a];
+                        dst[IDX(x, y, z) * 19 + OPP[a]] = f[a];
                     } else if ((sld == -1 && sld1 == -2) || sld == -2) {
                         if (bc_mode == 1 && flags[IDX(xt, yt, z)] != 0)
-                            scratch[IDX(x, y, z) * 19 + OPP[a]] = f[a];
+                            dst[IDX(x, y, z) * 19 + OPP[a]] = f[a];
                         else
-                            scratch[IDX(xt, yt, z) * 19 + MIR[a]] = f[a];
+                            dst[IDX(xt, yt, z) * 19 + MIR[a]] = f[a];
                     } else if (bc_mode == 1) {
                         /* solid inside the flow: halfway bounce-back */
-                        scratch[IDX(x, y, z) * 19 + OPP[a]] = f[a];
+                        dst[IDX(x, y, z) * 19 + OPP[a]] = f[a];
                     }
                 }
             }
         }
     }
+}
+
+int orc_step(int nx, int ny, int nz, double *state, double *scratch, const int8_t *flags,
+             double omega, double force, int bc_mode)
+{
     /* the reference swaps f/ftemp (xcomputations.c:557-559); copy back so the
-     * caller's buffer is the new state */
-    memcpy(state, scratch, (size_t)nx * ny * zd * 19 * sizeof(double));
+     * caller's buffer is the new state.  `scratch` must hold the previous
+     * contents of the destination (a copy of state is fine). */
+    orc_step_ab(nx, ny, nz, state, scratch, flags, omega, force, bc_mode);
+    memcpy(state, scratch, (size_t)nx * ny * (nz + 2) * 19 * sizeof(double));
+    return 0;
+}
+
+int orc_steps(int nx, int ny, int nz, double *state, double *scratch, const int8_t *flags, double omega,
+              double force, int bc_mode, long nsteps)
+{
+    /* alternate the two buffers (the reference's f/ftemp swap) and leave the
+     * result in `state` */
+    const size_t n = (size_t)nx * ny * (nz + 2) * 19;
+    double *a = state, *b = scratch;
+    memcpy(b, a, n * sizeof(double));
+    for (long s = 0; s < nsteps; s++) {
+        orc_step_ab(nx, ny, nz, a, b, flags, omega, force, bc_mode);
+        double *t = a; a = b; b = t;
+    }
+    if (a != state) memcpy(state, a, n * sizeof(double));
     return 0;
 }
 

@@ -44,6 +44,11 @@ enum {
 int orc_step(int nx, int ny, int nz, double *state, double *scratch, const int8_t *flags,
              double omega, double force, int bc_mode);
 
+/* nsteps steps at a fixed force without the per-step reductions (the
+ * two-buffer swap of xcomputations.c:557-559); result in `state`. */
+int orc_steps(int nx, int ny, int nz, double *state, double *scratch, const int8_t *flags, double omega,
+              double force, int bc_mode, long nsteps);
+
 /* encalc.c:3-146 restated; returns force = rho*ubulk - momentum and fills
  * out[ORC_LOG_RHO..ORC_LOG_MASSRATE]. */
 double orc_encalc(int nx, int ny, int nz, const double *state, double ubulk, double *out);

@@ -50,6 +50,7 @@ def lib():
         i8p = ctypes.POINTER(ctypes.c_int8)
         ci, cd, cl = ctypes.c_int, ctypes.c_double, ctypes.c_long
         L.orc_step.argtypes = [ci, ci, ci, dp, dp, i8p, cd, cd, ci]
+        L.orc_steps.argtypes = [ci, ci, ci, dp, dp, i8p, cd, cd, ci, cl]
         L.orc_encalc.argtypes = [ci, ci, ci, dp, cd, dp]
         L.orc_encalc.restype = cd
         L.orc_wshearstr.argtypes = [ci, ci, ci, dp, cd, cd, dp]
@@ -113,6 +114,14 @@ def step(state, flg, omega, force, bc_mode=0):
     nx, ny, nz = _dims(state)
     scratch = state.copy()
     lib().orc_step(nx, ny, nz, _dp(state), _dp(scratch), _i8(np.ascontiguousarray(flg, np.int8)), omega, force, bc_mode)
+
+
+def steps(state, flg, omega, force, nsteps, bc_mode=0):
+    """nsteps steps at a fixed force, populations only (no per-step logs)."""
+    nx, ny, nz = _dims(state)
+    scratch = np.empty_like(state)
+    lib().orc_steps(nx, ny, nz, _dp(state), _dp(scratch), _i8(np.ascontiguousarray(flg, np.int8)), omega, force,
+                    bc_mode, nsteps)
 
 
 def encalc(state, ubulk):

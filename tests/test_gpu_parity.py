@@ -193,3 +193,22 @@ def test_reference_ghost_flag_array(oracle_mod):
     ref = s0.copy()
     oracle_mod.run(ref, fl, 1.3, gx=1e-5, const_g=True, nsteps=6)
     np.testing.assert_array_equal(ch.store_state(), ref)
+
+
+@pytest.mark.parametrize("name", ["channel180", "grooves180"])
+def test_full_size_20_steps_bitexact(oracle_mod, name):
+    """The 20-step field check at full size: 628 x 202 x 314 (39.4M fluid
+    cells), Re_tau ~ 180, FP64, constant g, smooth walls and pitch-32 /
+    gas-fraction-0.5 longitudinal grooves; bit-identical to the oracle."""
+    wl = inputs.workload(name)
+    s0 = inputs.make_state(wl, seed=0)
+    fl = inputs.make_flags(wl)
+    with dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, gx=wl.gx, force_mode=dnslbm.CONST_G) as ch:
+        ch.set_flags(fl)
+        ch.load_state(s0)
+        ch.step(20)
+        got = ch.store_state()
+        logs = ch.logs()
+    assert np.isfinite(logs).all()
+    oracle_mod.steps(s0, fl, wl.omega, wl.gx, 20)  # in place
+    np.testing.assert_array_equal(got, s0)
