@@ -145,6 +145,33 @@ int dnslbm_sync(dnslbm_ctx *ctx);
 void *dnslbm_host_alloc(size_t bytes);
 void dnslbm_host_free(void *ptr);
 
+/* FP64 constant-g step that allocates nothing.  No counterpart in the
+ * reference: it is for callers that own all device memory through their own
+ * pool or arena and do not let a library call cudaMalloc.  The caller passes
+ * its populations in device memory -- 19 arrays of doubles, array a at
+ * pop + a*pop_stride, each holding cell (x, y, z) at (z*ydv + y)*xdv + x,
+ * z = 0..zdv-1 -- and they are advanced nsteps steps in place (the AA scheme
+ * of dnslbm_step).  parity is 0 when the populations are in this natural
+ * layout and 1 after an odd number of steps; it becomes (parity + nsteps) % 2.
+ * wallmask (device, may be NULL for smooth no-slip walls) holds per
+ * wall-adjacent cell, bottom plane then top plane, [2][ydv][xdv] bytes whose
+ * bits 0..4 mark the links with in-plane offsets (0,0) (1,0) (-1,0) (0,1)
+ * (0,-1) that bounce back (1) rather than reflect specularly (0).  logs
+ * (device, may be NULL) receives nsteps records of DNSLBM_LOG_N doubles.
+ * Work is queued on `stream` (NULL: the default stream) and the call returns
+ * without waiting; a NaN wall stress shows as NaN in the log records.
+ * Scratch lives in a fixed 1 MiB device array that every GPU loading the
+ * library holds until exit; a grid needs about 15 + 8*ceil(xdv/128) doubles
+ * of it per wall-normal plane (about 2400 planes at xdv = 628), and grids
+ * whose scratch does not fit are rejected with DNSLBM_ERR_ARG.
+ * All calls on a device share that array: calls that overlap on the GPU race.
+ * The first call on each device (made with the device that holds pop
+ * current) looks up the array's device address; make it before any stream
+ * capture.  err (may be NULL) receives a message on failure. */
+int dnslbm_step_f64_noalloc(double *pop, size_t pop_stride, int xdv, int ydv, int zdv, double omega, double gx,
+                            const uint8_t *wallmask, int parity, long nsteps, double *logs, void *stream, char *err,
+                            size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
