@@ -254,17 +254,19 @@ def run_ours(args):
     value = d.world * cells * args.steps / (tmax / 1e3) / 1e6
     bpc = ch.bytes_per_cell
     # dominant kernel: the parity with the larger summed device time
-    kbase = "step_f64_kernel" if args.precision == 64 else f"step_lp_kernel<fp{args.precision}>"
+    kdesc = ch.kernel
+    kbase = kdesc.split(" ")[0]
     if odd >= even:
-        kname, kms, kn = kbase + "<odd>", odd, n_odd
+        kname, kms, kn = kbase + " (odd parity)", odd, n_odd
     else:
-        kname, kms, kn = kbase + "<even>", even, n_even
+        kname, kms, kn = kbase + " (even parity)", even, n_even
     launch_s = kms / kn / 1e3
     achieved = bpc * cells / launch_s / 1e9
     traffic = ncu_traffic(f"{wl.name}:f{args.precision}")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": f"{peak_src} (MEASURED_PEAKS.json)",
-            "kernel": kname, "launch_ms": round(launch_s * 1e3, 4),
+            "kernel": kname, "kernel_config": kdesc, "launch_ms": round(launch_s * 1e3, 4),
+            "whole_step_frac": round(bpc * cells / (tmax / args.steps / 1e3) / 1e9 / peak, 4),
             "algorithmic_bytes_per_launch": bpc * cells, "bytes_per_cell": bpc}
 
     variants = {}

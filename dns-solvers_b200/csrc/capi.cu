@@ -20,6 +20,17 @@ void launch_reduce_lp(int precision, const StepArgs &p, dim3 grid, dim3 block, c
 void launch_io(int precision, int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s);
 void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int rows, int pass, const double *mean,
                   double *partials, double *plane_out, cudaStream_t s);
+struct TmaArgs {
+    int ngroups, groups_per_block, stages, row_bytes, k, gpp;
+};
+int tma_prepare_f64(size_t smem);
+int tma_occupancy_f64(int threads, size_t smem);
+void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, bool textured,
+                    cudaStream_t s);
+int tma_prepare_lp(int precision, size_t smem);
+int tma_occupancy_lp(int precision, int threads, size_t smem);
+void launch_tma_lp(int precision, const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd,
+                   bool textured, cudaStream_t s);
 }  // namespace dnslbm
 
 using namespace dnslbm;
@@ -27,6 +38,7 @@ using namespace dnslbm;
 struct dnslbm_ctx {
     dnslbm_deck deck;
     int nx, ny, nz;
+    int pitch;  // row pitch in elements: rows padded to 16 bytes for bulk copies
     size_t ncell, pstride, esize;
     void *popmem = nullptr;
     uint8_t *wallmask = nullptr;
@@ -42,6 +54,12 @@ struct dnslbm_ctx {
     std::vector<cudaEvent_t> tev;  // per-launch timing events
     dim3 grid, block;
     int rows = 8;
+    int slots = 1;  // partial-sum slots per plane
+    // row-pipelined (bulk-copy) step
+    int use_tma = 0, tma_threads = 0, tma_grid = 0;
+    char kernel_desc[160] = {0};
+    size_t tma_smem = 0;
+    TmaArgs tma{};
     int have_state = 0;
     int odd = 0;  // parity of the next step (1: populations are post-collision, swapped)
     long long done = 0;
@@ -73,7 +91,9 @@ static StepArgs step_args(const dnslbm_ctx *c)
     p.nx = c->nx;
     p.ny = c->ny;
     p.nz = c->nz;
+    p.pitch = c->pitch;
     p.rows = c->rows;
+    p.slots = c->slots;
     p.wallmask = c->wallmask;
     p.omega = c->deck.omega;
     p.ubulk = c->deck.ubulk;
@@ -99,6 +119,7 @@ static IoArgs io_args(const dnslbm_ctx *c)
     p.nx = c->nx;
     p.ny = c->ny;
     p.nz = c->nz;
+    p.pitch = c->pitch;
     p.wallmask = c->wallmask;
     p.textured = c->textured;
     p.odd = c->odd;
@@ -128,7 +149,7 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     if (deck->xdv < 2 || deck->ydv < 2 || deck->zdv < 3)
         return fail(c, DNSLBM_ERR_ARG, "grid %dx%dx%d too small (need xdv,ydv >= 2, zdv >= 3)", deck->xdv, deck->ydv,
                     deck->zdv);
-    if ((long long)deck->xdv * deck->ydv * deck->zdv >= (1LL << 31))
+    if ((long long)(deck->xdv + 8) * deck->ydv * deck->zdv >= (1LL << 31))
         return fail(c, DNSLBM_ERR_ARG, "grid of %lld cells exceeds 2^31", (long long)deck->xdv * deck->ydv * deck->zdv);
     if (!(deck->omega > 0.0 && deck->omega < 2.0)) return fail(c, DNSLBM_ERR_ARG, "omega %g outside (0,2)", deck->omega);
     if (deck->precision != 64 && deck->precision != 32 && deck->precision != 16)
@@ -145,8 +166,15 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     c->nx = deck->xdv;
     c->ny = deck->ydv;
     c->nz = deck->zdv;
-    c->ncell = (size_t)c->nx * c->ny * c->nz;
     c->esize = deck->precision / 8;
+    {
+        // rows start on `align` bytes (16 at least, for the bulk copies)
+        int align_bytes = 32;
+        if (const char *e = getenv("DNSLBM_ROW_ALIGN")) align_bytes = std::max(16, atoi(e));
+        const int v = align_bytes / (int)c->esize;
+        c->pitch = (c->nx + v - 1) / v * v;
+    }
+    c->ncell = (size_t)c->pitch * c->ny * c->nz;
     const size_t align = 256 / c->esize;
     c->pstride = (c->ncell + align - 1) / align * align;
 
@@ -166,7 +194,68 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     if (bx > 128) bx = 128;
     c->block = dim3(bx, 1, 1);
     c->grid = dim3((c->nx + bx - 1) / bx, (c->ny + c->rows - 1) / c->rows, c->nz);
-    const size_t nblocks = (size_t)c->grid.x * c->grid.y * c->grid.z;
+    c->slots = (int)(c->grid.x * c->grid.y);
+    {
+        // row-pipelined step: whole rows through shared memory, `stages`
+        // rows in flight per block; used when two stages fit
+        const char *path = getenv("DNSLBM_PATH");
+        const int row_bytes = c->pitch * (int)c->esize;
+        // A stage holds a group of k consecutive rows of one plane for all 19
+        // directions.  Defaults measured on a B200 (628-wide rows): two
+        // stages of about 48 KB (FP16) to 96 KB (FP32/FP64) per block, whole
+        // rows per consumer thread pair; FP16 runs two blocks per SM.
+        const size_t stage_target = c->deck.precision == 16 ? 49152 : 98304;
+        int k = 1;
+        while (k < 8 && k * 2 <= c->ny && (size_t)Q * row_bytes * k * 2 <= stage_target) k *= 2;
+        if (const char *e = getenv("DNSLBM_GROUP_ROWS")) k = std::max(1, std::min(atoi(e), c->ny));
+        const size_t smem_stage = (size_t)Q * row_bytes * k;
+        int maxsmem = 0, nsm = 0;
+        cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, deck->device);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, deck->device);
+        int stages = 2;
+        if (const char *e = getenv("DNSLBM_STAGES")) stages = atoi(e);
+        while (stages > 2 && (size_t)stages * smem_stage + 16 * (size_t)stages > (size_t)maxsmem) --stages;
+        const size_t smem = (size_t)stages * smem_stage + 16 * (size_t)stages;  // + full/empty mbarriers
+        const bool fits = stages >= 2 && smem <= (size_t)maxsmem && nsm > 0;
+        if (fits && !(path && !strcmp(path, "scalar"))) {
+            // consumer threads: about 2 cells each along the row, at most 352
+            int cpt = (c->nx + 319) / 320;
+            int consumers = ((c->nx + cpt - 1) / cpt + 31) / 32 * 32;
+            if (c->deck.precision == 16) consumers = std::min(consumers, 128);  // two blocks per SM
+            if (const char *e = getenv("DNSLBM_THREADS")) consumers = atoi(e) / 32 * 32;
+            if (consumers > 352) consumers = 352;
+            if (consumers < 32) consumers = 32;
+            const int threads = consumers + 32;
+            int prep = c->deck.precision == 64 ? tma_prepare_f64(smem) : tma_prepare_lp(c->deck.precision, smem);
+            int occ = prep ? 0
+                           : (c->deck.precision == 64 ? tma_occupancy_f64(threads, smem)
+                                                      : tma_occupancy_lp(c->deck.precision, threads, smem));
+            if (const char *e = getenv("DNSLBM_BLOCKS_PER_SM")) occ = std::min(occ, atoi(e));
+            if (occ >= 1) {
+                const int gpp = (c->ny + k - 1) / k, ngroups = gpp * c->nz;
+                const int target = occ * nsm;
+                const int GB = (ngroups + target - 1) / target;
+                c->use_tma = 1;
+                c->tma_threads = threads;
+                c->tma_smem = smem;
+                c->tma_grid = (ngroups + GB - 1) / GB;
+                c->tma = TmaArgs{ngroups, GB, stages, row_bytes, k, gpp};
+                c->slots = std::max(c->slots, (gpp + GB - 1) / GB + 1);
+            }
+        }
+        cudaGetLastError();  // an attribute query that failed only selects the scalar path
+    }
+    if (c->use_tma)
+        snprintf(c->kernel_desc, sizeof c->kernel_desc,
+                 "step_tma_kernel<fp%d> row-pipelined bulk-copy: %d blocks x %d threads, %d groups of %d rows/block, "
+                 "%d stages, %zu B smem",
+                 c->deck.precision, c->tma_grid, c->tma_threads, c->tma.groups_per_block, c->tma.k, c->tma.stages,
+                 c->tma_smem);
+    else
+        snprintf(c->kernel_desc, sizeof c->kernel_desc, "%s per-thread: grid %ux%ux%u x %u threads",
+                 c->deck.precision == 64 ? "step_f64_kernel" : "step_lp_kernel", c->grid.x, c->grid.y, c->grid.z,
+                 c->block.x);
+    const size_t nblocks = (size_t)c->nz * c->slots;
 
     struct Alloc { void **p; size_t bytes; };
     c->staging_bytes = std::min<size_t>((size_t)256 << 20, (size_t)c->ny * (c->nz + 2) * Q * sizeof(double) * c->nx);
@@ -310,6 +399,8 @@ static int initial_reduce(dnslbm_ctx *c)
 
 static int reset_counters(dnslbm_ctx *c)
 {
+    CK(cudaMemsetAsync(c->plane_ctr, 0, (size_t)c->nz * sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->total_ctr, 0, sizeof(unsigned), c->stream));
     CK(cudaMemsetAsync(c->step_ctr, 0, sizeof(long long), c->stream));
     CK(cudaMemsetAsync(c->status, 0, 2 * sizeof(long long), c->stream));
     CK(cudaMemsetAsync(c->shift, 0, (size_t)2 * c->nz * 3 * sizeof(double), c->stream));
@@ -385,8 +476,17 @@ static int launch_steps(dnslbm_ctx *c, long n, bool timed, double *ms_even, doub
     for (long s = 0; s < n; ++s) {
         const bool odd = c->odd != 0;
         if (timed) CK(cudaEventRecord(c->tev[2 * s], c->stream));
-        if (c->deck.precision == 64) launch_step_f64(p, c->grid, c->block, odd, c->textured != 0, c->stream);
-        else launch_step_lp(c->deck.precision, p, c->grid, c->block, odd, c->textured != 0, c->stream);
+        if (c->use_tma) {
+            if (c->deck.precision == 64)
+                launch_tma_f64(p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd, c->textured != 0, c->stream);
+            else
+                launch_tma_lp(c->deck.precision, p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd,
+                              c->textured != 0, c->stream);
+        } else if (c->deck.precision == 64) {
+            launch_step_f64(p, c->grid, c->block, odd, c->textured != 0, c->stream);
+        } else {
+            launch_step_lp(c->deck.precision, p, c->grid, c->block, odd, c->textured != 0, c->stream);
+        }
         CK(cudaGetLastError());
         if (timed) CK(cudaEventRecord(c->tev[2 * s + 1], c->stream));
         c->odd ^= 1;
@@ -408,6 +508,7 @@ static int check_status(dnslbm_ctx *c)
     long long st[2];
     CK(cudaMemcpyAsync(st, c->status, sizeof st, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (st[1]) return fail(c, DNSLBM_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out; state invalid, reload it");
     if (st[0]) return fail(c, DNSLBM_ERR_NAN, "NaN wall shear stress at step %lld", st[0] - 1);
     return DNSLBM_OK;
 }
@@ -541,6 +642,8 @@ extern "C" int dnslbm_statistics(dnslbm_ctx *c, double *out)
     }
     return DNSLBM_OK;
 }
+
+extern "C" const char *dnslbm_step_kernel(const dnslbm_ctx *c) { return c ? c->kernel_desc : ""; }
 
 extern "C" double dnslbm_bytes_per_cell(const dnslbm_ctx *c) { return c ? 2.0 * Q * (double)c->esize : 0.0; }
 

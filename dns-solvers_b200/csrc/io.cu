@@ -45,12 +45,12 @@ template <typename T>
 __device__ __forceinline__ void gather_natural(const IoArgs &p, int x, int y, int z, double (&f)[Q])
 {
     if (!p.odd) {
-        const int c = (z * p.ny + y) * p.nx + x;
+        const int c = (z * p.ny + y) * p.pitch + x;
 #pragma unroll
         for (int a = 0; a < Q; ++a) f[a] = Nat<T>::ld(static_cast<const T *>(p.pop[a]) + c, a);
         return;
     }
-    const Nbr n = make_nbr(x, y, z, p.nx, p.ny);
+    const Nbr n = make_nbr(x, y, z, p.nx, p.ny, p.pitch);
     const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
     unsigned bits = 0x1fu;
     if (p.textured && wall != 0) bits = p.wallmask[(size_t)(wall > 0) * p.nx * p.ny + y * p.nx + x];
@@ -95,17 +95,17 @@ __global__ void import_kernel(const IoArgs p, int x0, int nxc, const double *aos
     const int y = (int)((tid / p.nz) % p.ny);
     const int xl = (int)(tid / ((long long)p.nz * p.ny));
     const double *i = aos + (((size_t)xl * p.ny + y) * (p.nz + 2) + (z + 1)) * Q;
-    const int c = (z * p.ny + y) * p.nx + (x0 + xl);
+    const int c = (z * p.ny + y) * p.pitch + (x0 + xl);
 #pragma unroll
     for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, i[a], a);
 }
 
-// rest state f = w (init.c:6-19)
+// rest state f = w (init.c:6-19); row padding included
 template <typename T>
 __global__ void rest_kernel(const IoArgs p)
 {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= (long long)p.nx * p.ny * p.nz) return;
+    if (c >= (long long)p.pitch * p.ny * p.nz) return;
 #pragma unroll
     for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, Nat<float>::wq(a), a);
 }
@@ -233,7 +233,7 @@ static void io_dispatch(int what, const IoArgs &p, int x0, int nxc, double *a, d
         const long long n = (long long)nxc * p.ny * p.nz;
         import_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p, x0, nxc, a);
     } else if (what == 2) {
-        const long long n = (long long)p.nx * p.ny * p.nz;
+        const long long n = (long long)p.pitch * p.ny * p.nz;
         rest_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p);
     } else {
         const long long n = (long long)nxc * p.ny * (p.nz + 2);

@@ -149,7 +149,9 @@ extern "C" int dnslbm_step_f64_noalloc(double *pop, size_t pop_stride, int xdv, 
     p.nx = xdv;
     p.ny = ydv;
     p.nz = zdv;
+    p.pitch = xdv;  // the caller's rows are unpadded
     p.rows = rows;
+    p.slots = ((xdv + bx - 1) / bx) * ((ydv + rows - 1) / rows);
     p.wallmask = wallmask;
     p.omega = omega;
     p.ubulk = 0.0;

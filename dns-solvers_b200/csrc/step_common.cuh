@@ -22,14 +22,16 @@ constexpr int NP = 8;
 struct StepArgs {
     void *pop[Q];            // population arrays (slot a)
     int nx, ny, nz;
-    int rows;                // rows (y) per block
+    int pitch;               // row pitch in elements (>= nx)
+    int rows;                // rows (y) per block (scalar kernels)
+    int slots;               // partial-sum slots per plane
     const uint8_t *wallmask; // [2][ny][nx] wall-link bits (bottom, top)
     double omega, ubulk, gx;
     int const_q;
     double *force;           // [2] force of step s is force[s & 1]
     double *shift;           // [2][nz][3] plane means of the previous state
     long long *step_ctr;     // steps done (advanced by the step tail)
-    double *partials;        // [blocks][NP]
+    double *partials;        // [nz][slots][NP]
     double *plane_sums;      // [nz][NP]
     unsigned *plane_ctr;     // [nz]
     unsigned *total_ctr;     // [1]
@@ -42,6 +44,7 @@ struct StepArgs {
 struct IoArgs {
     void *pop[Q];
     int nx, ny, nz;
+    int pitch;  // row pitch in elements
     const uint8_t *wallmask;
     int textured;
     int odd;  // 1: populations are post-collision in swapped slots
@@ -51,11 +54,11 @@ struct IoArgs {
 // Neighbourhood of a cell: wrapped x and the 9 row offsets (dy, dz).
 struct Nbr {
     int x, xm, xp;
-    int row[3][3];  // row[dy+1][dz+1] = ((z+dz)*ny + wrap(y+dy))*nx
+    int row[3][3];  // row[dy+1][dz+1] = ((z+dz)*ny + wrap(y+dy))*pitch
     int c0;         // own cell
 };
 
-__device__ __forceinline__ Nbr make_nbr(int x, int y, int z, int nx, int ny)
+__device__ __forceinline__ Nbr make_nbr(int x, int y, int z, int nx, int ny, int pitch)
 {
     Nbr n;
     n.x = x;
@@ -67,7 +70,7 @@ __device__ __forceinline__ Nbr make_nbr(int x, int y, int z, int nx, int ny)
 #pragma unroll
     for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-        for (int dz = 0; dz < 3; ++dz) n.row[dy][dz] = ((z + dz - 1) * ny + ys[dy]) * nx;
+        for (int dz = 0; dz < 3; ++dz) n.row[dy][dz] = ((z + dz - 1) * ny + ys[dy]) * pitch;
     n.c0 = n.row[1][1] + x;
     return n;
 }
@@ -115,24 +118,40 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV])
         for (int i = 0; i < NV; ++i) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
 }
 
-// Deterministic block sum (fixed shuffle tree, warps added in order); the
-// result is valid in thread 0.  smem holds 32*NV doubles.
+// Barrier over the first `nthreads` threads of the block (all of them when
+// nthreads == blockDim.x): named barrier 1, so a producer warp outside the
+// group never has to take part.
+__device__ __forceinline__ void group_sync(int nthreads)
+{
+    if (nthreads == (int)blockDim.x) __syncthreads();
+    else asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Deterministic sum over the first `nthreads` threads (fixed shuffle tree,
+// warps added in order); the result is valid in thread 0.  smem holds
+// 32*NV doubles.
 template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem)
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem, int nthreads)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nwarp = (blockDim.x + 31) >> 5;
+    const int nwarp = (nthreads + 31) >> 5;
     warp_sum<NV>(v);
-    __syncthreads();
+    group_sync(nthreads);
     if (lane == 0)
 #pragma unroll
         for (int i = 0; i < NV; ++i) smem[warp * NV + i] = v[i];
-    __syncthreads();
+    group_sync(nthreads);
     if (warp == 0) {
 #pragma unroll
         for (int i = 0; i < NV; ++i) v[i] = lane < nwarp ? smem[lane * NV + i] : 0.0;
         warp_sum<NV>(v);
     }
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem)
+{
+    block_sum<NV>(v, smem, blockDim.x);
 }
 
 // Final step tail, run by the last block of the launch: plane sums ->
@@ -141,14 +160,15 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *smem)
 // mode 0: after a step (logs, advances the step counter);
 // mode 1: initial reduction of a freshly loaded state (force and shift of
 //         the current step from the reader-side totals, nothing logged).
-static __device__ __forceinline__ void step_tail(const StepArgs &a, long long step, double force_used, int mode, double *smem)
+static __device__ __forceinline__ void step_tail(const StepArgs &a, long long step, double force_used, int mode, double *smem,
+                                                 int nthreads)
 {
     const int nz = a.nz;
     const double np = (double)a.nx * (double)a.ny;
     const double *cshift = a.shift + (size_t)(step & 1) * nz * 3;
     double *nshift = a.shift + (size_t)((mode == 0 ? step + 1 : step) & 1) * nz * 3;
     double t[6] = {0, 0, 0, 0, 0, 0};  // rho, jx, sum of plane means u, K, writer rho, writer jx
-    for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    for (int z = threadIdx.x; z < nz; z += nthreads) {
         const double *ps = a.plane_sums + (size_t)z * NP;
         double s[NP];
 #pragma unroll
@@ -165,7 +185,7 @@ static __device__ __forceinline__ void step_tail(const StepArgs &a, long long st
         nshift[z * 3 + 1] = vm;
         nshift[z * 3 + 2] = wm;
     }
-    block_sum<6>(t, smem);
+    block_sum<6>(t, smem, nthreads);
     if (threadIdx.x != 0) return;
     const double N = np * (double)nz;
     const double rho = t[0] / N, momentum = t[1] / N;
@@ -200,38 +220,37 @@ static __device__ __forceinline__ void step_tail(const StepArgs &a, long long st
     *a.step_ctr = step + 1;
 }
 
-// Block epilogue of every fused kernel: block partials -> (last block of the
-// plane) plane sums -> (last plane) step tail.  No block waits for another:
-// the last arrival does the work, found with atomic tickets.
-__device__ __forceinline__ void block_epilogue(const StepArgs &a, double (&acc)[NP], long long step, double force_used,
-                                               int mode)
+// One block's contribution to plane z: block partials -> (last contributor
+// of the plane) plane sums in a fixed order -> (last plane) step tail.  No
+// block waits for another: the last arrival does the work, found with atomic
+// tickets.  `slot` numbers the block among the `ncontrib` contributors of
+// the plane; the call is block-uniform.
+__device__ __forceinline__ void plane_contribute(const StepArgs &a, double (&acc)[NP], int z, int slot, int ncontrib,
+                                                 long long step, double force_used, int mode, int nthreads)
 {
     __shared__ double smem[32 * NP];
     __shared__ unsigned ticket;
-    block_sum<NP>(acc, smem);
-    const unsigned bpp = gridDim.x * gridDim.y;
-    const unsigned bid = blockIdx.y * gridDim.x + blockIdx.x;
-    const int z = blockIdx.z;
+    block_sum<NP>(acc, smem, nthreads);
     if (threadIdx.x == 0) {
-        double *p = a.partials + ((size_t)z * bpp + bid) * NP;
+        double *p = a.partials + ((size_t)z * a.slots + slot) * NP;
 #pragma unroll
         for (int i = 0; i < NP; ++i) p[i] = acc[i];
         __threadfence();
         ticket = atomicAdd(a.plane_ctr + z, 1u);
     }
-    __syncthreads();
-    if (ticket != bpp - 1) return;
-    // last block of plane z: fixed-order plane sum
+    group_sync(nthreads);
+    if (ticket != (unsigned)ncontrib - 1) return;
+    // last contributor of plane z: fixed-order plane sum
     __threadfence();
     double s[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) s[i] = 0.0;
-    for (unsigned b = threadIdx.x; b < bpp; b += blockDim.x) {
-        const double *p = a.partials + ((size_t)z * bpp + b) * NP;
+    for (int b = threadIdx.x; b < ncontrib; b += nthreads) {
+        const double *p = a.partials + ((size_t)z * a.slots + b) * NP;
 #pragma unroll
         for (int i = 0; i < NP; ++i) s[i] += __ldcg(p + i);
     }
-    block_sum<NP>(s, smem);
+    block_sum<NP>(s, smem, nthreads);
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int i = 0; i < NP; ++i) a.plane_sums[(size_t)z * NP + i] = s[i];
@@ -239,11 +258,21 @@ __device__ __forceinline__ void block_epilogue(const StepArgs &a, double (&acc)[
         __threadfence();
         ticket = atomicAdd(a.total_ctr, 1u);
     }
-    __syncthreads();
+    group_sync(nthreads);
     if (ticket != (unsigned)a.nz - 1) return;
     __threadfence();
-    step_tail(a, step, force_used, mode, smem);
+    step_tail(a, step, force_used, mode, smem, nthreads);
     if (threadIdx.x == 0) *a.total_ctr = 0;
+    group_sync(nthreads);
+}
+
+// Epilogue of the scalar kernels: one block per (x-chunk, row-chunk) of a
+// plane, blockIdx.z = plane.
+__device__ __forceinline__ void block_epilogue(const StepArgs &a, double (&acc)[NP], long long step, double force_used,
+                                               int mode)
+{
+    const int bpp = gridDim.x * gridDim.y;
+    plane_contribute(a, acc, blockIdx.z, blockIdx.y * gridDim.x + blockIdx.x, bpp, step, force_used, mode, blockDim.x);
 }
 
 }  // namespace dnslbm

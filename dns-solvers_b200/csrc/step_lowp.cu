@@ -1,68 +1,14 @@
-// Reduced-precision fused step: populations stored as deviations
-// d_a = f_a - w_a (rho0 = 1) in FP32 or FP16 and collided in FP32.
-// FP16 values carry a scale of 2^15 (exact, a power of two) so deviations of
-// 1e-7..2 stay in the normal range of binary16.  The per-step reductions, the
-// constant-Q force update and the statistics are accumulated in FP64.
-//
-// The collision is the reference's (xcomputations.c:314-342) rewritten for
-// deviations: with dr = sum d_a, rho = 1 + dr, u = j / rho,
-//   feq_a - w_a = w_a (dr + rho (3 e.u + 4.5 (e.u)^2 - 1.5 u.u))
-//   d_a' = d_a + Fi_a - omega (d_a - (feq_a - w_a)),
-//   Fi_a = w_a (3 (e_x - u_x) + 9 (e.u) e_x) G.
+// Reduced-precision fused step with per-thread global accesses (one thread
+// per cell): populations stored as deviations f_a - w_a in FP32 or FP16
+// (collide_lp.cuh), collided in FP32; the per-step reductions and the
+// constant-Q force are accumulated in FP64.  Used where the row-pipelined
+// kernel (step_tma.cuh) does not fit shared memory.
 #include <cuda_fp16.h>
 
+#include "collide_lp.cuh"
 #include "step_common.cuh"
 
 namespace dnslbm {
-
-template <typename T> struct DevStore;
-template <> struct DevStore<float> {
-    static __device__ __forceinline__ float ld(const float *p) { return *p; }
-    static __device__ __forceinline__ void st(float *p, float v) { *p = v; }
-};
-template <> struct DevStore<__half> {
-    static constexpr float kScale = 32768.f, kInv = 1.f / 32768.f;
-    static __device__ __forceinline__ float ld(const __half *p) { return __half2float(*p) * kInv; }
-    static __device__ __forceinline__ void st(__half *p, float v) { *p = __float2half_rn(v * kScale); }
-};
-
-__host__ __device__ __forceinline__ constexpr float lat_w(int a)
-{
-    return a == 0 ? 1.f / 3.f : a <= 6 ? 1.f / 18.f : 1.f / 36.f;
-}
-
-struct LpCell {
-    float rho, jx, u0, u1, u2;
-};
-
-__device__ __forceinline__ LpCell lp_collide(float (&d)[Q], float omega, float G)
-{
-    float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-    for (int a = 0; a < Q; ++a) {
-        dr += d[a];
-        if (lat_ex(a)) jx += lat_ex(a) > 0 ? d[a] : -d[a];
-        if (lat_ey(a)) jy += lat_ey(a) > 0 ? d[a] : -d[a];
-        if (lat_ez(a)) jz += lat_ez(a) > 0 ? d[a] : -d[a];
-    }
-    LpCell c;
-    c.rho = 1.f + dr;
-    const float inv = 1.f / c.rho;
-    c.jx = jx;
-    c.u0 = jx * inv;
-    c.u1 = jy * inv;
-    c.u2 = jz * inv;
-    const float usq15 = 1.5f * (c.u0 * c.u0 + c.u1 * c.u1 + c.u2 * c.u2);
-    const float om1 = 1.f - omega;
-#pragma unroll
-    for (int a = 0; a < Q; ++a) {
-        const float eu = (float)lat_ex(a) * c.u0 + (float)lat_ey(a) * c.u1 + (float)lat_ez(a) * c.u2;
-        const float feqd = lat_w(a) * (dr + c.rho * (3.f * eu + 4.5f * eu * eu - usq15));
-        const float Fi = lat_w(a) * (3.f * ((float)lat_ex(a) - c.u0) + 9.f * eu * (float)lat_ex(a)) * G;
-        d[a] = om1 * d[a] + omega * feqd + Fi;
-    }
-    return c;
-}
 
 template <typename T, int A, bool ODD>
 __device__ __forceinline__ T *lp_ptr(const StepArgs &p, const Nbr &n, int wall, unsigned bits)
@@ -75,7 +21,8 @@ __device__ __forceinline__ T *lp_ptr(const StepArgs &p, const Nbr &n, int wall, 
 template <typename T, bool ODD, bool CONSTQ, bool TEXTURED>
 __global__ void __launch_bounds__(128, 4) step_lp_kernel(const StepArgs p)
 {
-    using S = DevStore<T>;
+    using S = LpStore<T>;
+    constexpr float iS = S::kInv;
     const long long step = *p.step_ctr;
     const double Gd = CONSTQ ? p.force[step & 1] : p.gx;
     const float G = (float)Gd;
@@ -92,7 +39,7 @@ __global__ void __launch_bounds__(128, 4) step_lp_kernel(const StepArgs p)
         const int y0 = blockIdx.y * p.rows;
         const int y1 = min(y0 + p.rows, p.ny);
         for (int y = y0; y < y1; ++y) {
-            const Nbr n = make_nbr(x, y, z, p.nx, p.ny);
+            const Nbr n = make_nbr(x, y, z, p.nx, p.ny, p.pitch);
             unsigned bits = 0x1fu;
             if (TEXTURED && wall != 0) bits = p.wallmask[(size_t)(wall > 0) * p.nx * p.ny + y * p.nx + x];
             float d[Q];
@@ -107,15 +54,15 @@ __global__ void __launch_bounds__(128, 4) step_lp_kernel(const StepArgs p)
                 }
                 d[ODD ? lat_opp(a) : a] = S::ld(q);
             }
-            const LpCell c = lp_collide(d, p.omega, G);
-            acc[0] += (double)c.rho;
+            const LpCell c = lp_collide<T>(d, p.omega, G);
+            acc[0] += 1.0 + (double)c.drho;
             acc[1] += (double)c.jx;
             acc[2] += (double)c.u0;
             acc[3] += (double)c.u1;
             acc[4] += (double)c.u2;
             {
-                const double d0 = c.u0 - c0, d1 = c.u1 - c1, d2 = c.u2 - c2;
-                acc[5] += d0 * d0 + d1 * d1 + d2 * d2;
+                const float d0 = c.u0 - (float)c0, d1 = c.u1 - (float)c1, d2 = c.u2 - (float)c2;
+                acc[5] += (double)(d0 * d0 + d1 * d1 + d2 * d2);
             }
             if (CONSTQ) {
                 float s = 0.f, m = 0.f;
@@ -124,12 +71,14 @@ __global__ void __launch_bounds__(128, 4) step_lp_kernel(const StepArgs p)
                     s += d[a];
                     if (lat_ex(a)) m += lat_ex(a) > 0 ? d[a] : -d[a];
                 }
+                s *= iS;
+                m *= iS;
                 if (wall != 0) {
                     const int ap = wall < 0 ? 12 : 11, am = wall < 0 ? 13 : 14;
                     // a bounced link arrives with e_x reversed; its weight
                     // part w_a contributes -2 e_x w_a too
-                    if (bits & 2u) m -= 2.f * (d[ap] + 1.f / 36.f);
-                    if (bits & 4u) m += 2.f * (d[am] + 1.f / 36.f);
+                    if (bits & 2u) m -= 2.f * (d[ap] * iS + 1.f / 36.f);
+                    if (bits & 4u) m += 2.f * (d[am] * iS + 1.f / 36.f);
                 }
                 acc[6] += 1.0 + (double)s;
                 acc[7] += (double)m;
@@ -153,7 +102,8 @@ __global__ void __launch_bounds__(128, 4) step_lp_kernel(const StepArgs p)
 template <typename T>
 __global__ void __launch_bounds__(128) reduce_lp_kernel(const StepArgs p)
 {
-    using S = DevStore<T>;
+    using S = LpStore<T>;
+    constexpr float iS = S::kInv;
     const long long step = *p.step_ctr;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.z;
@@ -164,11 +114,11 @@ __global__ void __launch_bounds__(128) reduce_lp_kernel(const StepArgs p)
         const int y0 = blockIdx.y * p.rows;
         const int y1 = min(y0 + p.rows, p.ny);
         for (int y = y0; y < y1; ++y) {
-            const int c = (z * p.ny + y) * p.nx + x;
+            const int c = (z * p.ny + y) * p.pitch + x;
             float dr = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
 #pragma unroll
             for (int a = 0; a < Q; ++a) {
-                const float v = S::ld(static_cast<const T *>(p.pop[a]) + c);
+                const float v = S::ld(static_cast<const T *>(p.pop[a]) + c) * iS;
                 dr += v;
                 if (lat_ex(a)) jx += lat_ex(a) > 0 ? v : -v;
                 if (lat_ey(a)) jy += lat_ey(a) > 0 ? v : -v;

@@ -1,0 +1,451 @@
+// Row-pipelined fused step on the Blackwell bulk-copy engine.
+//
+// A block owns a contiguous range of cell rows (y, z) (x runs along the
+// row).  In the AA scheme the 19 addresses of a cell are, per direction A,
+// one element of one population row: for the whole cell row they are 19
+// complete rows of the population arrays (row (y+ey, z+ez) of slot A in an
+// odd step, row (y, z) of slot A in an even step), which no other cell row
+// touches.  The block is warp-specialised:
+//   * the last warp is the producer: lane A moves direction A's row --
+//     a cp.async.bulk load into a shared-memory stage (completing on the
+//     stage's "full" mbarrier), and, once the consumers release the stage
+//     (its "empty" mbarrier), the cp.async.bulk store of the updated row;
+//     `stages` rows are in flight per block;
+//   * the other warps are consumers: they collide every cell of the row,
+//     reading direction A at x + ex (the periodic wrap in x is a
+//     shared-memory index) and writing the result back to the same
+//     shared-memory element, then release the stage.
+// Rows are padded to a 16-byte pitch so every copy is aligned.  No consumer
+// computes a global address on the interior path, and no consumer ever waits
+// for the producer's copy issue or store completion.
+//
+// Wall rows of an odd step: with smooth walls a link into the wall bounces
+// back to the cell's own slot opp(A), again a whole own row (bulk).  With a
+// textured wall the five links into the wall go to rows that several cell
+// rows share (bounce-back or specular per cell), so those five are moved by
+// per-thread loads/stores and never by a bulk copy.
+//
+// Every wait on an mbarrier is bounded; a wait that runs out records
+// status[1] and a shared abort flag, after which no thread of the block waits
+// again (the host reports DNSLBM_ERR_TIMEOUT).
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
+#include "collide_f64.cuh"
+#include "collide_lp.cuh"
+#include "step_common.cuh"
+
+namespace dnslbm {
+
+struct TmaArgs {
+    int ngroups;          // row groups: nz * gpp
+    int groups_per_block; // contiguous row groups per block
+    int stages;           // row groups in flight per block
+    int row_bytes;        // pitch * sizeof(storage)
+    int k;                // cell rows per group (consecutive y of one plane)
+    int gpp;              // groups per plane, ceil(ny / k)
+};
+
+// ------------------------------------------------------------------ PTX
+__device__ __forceinline__ uint32_t sm_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sm_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(sm_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     sm_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(sm_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(sm_addr(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+constexpr int kWaitLimit = 1 << 22;  // try_wait rounds before a wait is declared lost
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    for (int i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// ------------------------------------------------------------------ rows
+// Row group g = cell rows y0 .. y0+k-1 of plane z.  Direction A's
+// shared-memory block holds the k population rows of A's address set, in
+// order of the cell rows: rows y0+j+ey (periodic in y) of plane z+ez and slot
+// A in an odd step, rows y0+j of plane z and slot A in an even step, or the
+// cell rows' own rows of slot opp(A) for a smooth-wall bounce-back.  In
+// memory they are contiguous except where the y index wraps, so a direction
+// needs one copy, or two at the wrap.  `bulk` is false for the textured wall
+// links of an odd step, which move per thread.
+struct GroupRows {
+    int slot, zz;     // population array and plane of the rows
+    int y_first;      // first source row (j = 0), before wrapping
+    bool bulk;
+};
+
+template <bool ODD, bool TEXTURED>
+__device__ __forceinline__ GroupRows group_rows(const StepArgs &p, int A, int y0, int z, int wall)
+{
+    GroupRows g;
+    const int ez = lat_ez(A);
+    g.bulk = true;
+    if (!ODD) {
+        g.slot = A; g.zz = z; g.y_first = y0;
+    } else if (ez != 0 && ez == wall) {
+        g.bulk = !TEXTURED;
+        g.slot = lat_opp(A); g.zz = z; g.y_first = y0;  // bounce-back to the cell's own rows
+    } else {
+        g.slot = A; g.zz = z + ez; g.y_first = y0 + lat_ey(A);
+    }
+    return g;
+}
+
+// Issue the copies of one direction's rows (load: to_smem, else store).
+template <typename T>
+__device__ __forceinline__ void copy_group(const StepArgs &p, const TmaArgs &t, const GroupRows &g, int k,
+                                           unsigned char *sdir, bool to_smem, uint64_t *bar)
+{
+    const int ny = p.ny;
+    const size_t rb = (size_t)t.row_bytes;
+    auto one = [&](int ysrc, int j, int nrows) {
+        T *gp = static_cast<T *>(p.pop[g.slot]) + (size_t)(g.zz * ny + ysrc) * p.pitch;
+        unsigned char *sp = sdir + (size_t)j * rb;
+        if (to_smem) bulk_g2s(sp, gp, (uint32_t)(nrows * rb), bar);
+        else bulk_s2g(gp, sp, (uint32_t)(nrows * rb));
+    };
+    const int y = g.y_first;
+    if (y < 0) {                    // j = 0 wraps to the last row
+        one(ny - 1, 0, 1);
+        if (k > 1) one(0, 1, k - 1);
+    } else if (y + k > ny) {        // the last j wraps to row 0 (y <= ny)
+        if (ny - y > 0) one(y, 0, ny - y);
+        one(0, ny - y, k - (ny - y));
+    } else {
+        one(y, 0, k);
+    }
+}
+
+// ------------------------------------------------------------------ cells
+template <typename T>
+using RegT = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
+
+template <typename T>
+__device__ __forceinline__ RegT<T> ld_raw(const T *q)
+{
+    if constexpr (std::is_same<T, double>::value) return *q;
+    else return LpStore<T>::ld(q);
+}
+template <typename T>
+__device__ __forceinline__ void st_raw(T *q, RegT<T> v)
+{
+    if constexpr (std::is_same<T, double>::value) *q = v;
+    else LpStore<T>::st(q, v);
+}
+
+// One cell row from the stage buffer: direction A's element x at
+// sb[A * dstride + x].
+// WALL: 0 interior plane, -1 bottom plane, +1 top plane.
+template <typename T, bool ODD, bool CONSTQ, bool TEXTURED, int WALL>
+__device__ __forceinline__ void tma_row(const StepArgs &p, T *sb, int dstride, int y, int z, double G,
+                                        const double *shift, double (&acc)[NP], int nc)
+{
+    using V = RegT<T>;
+    const double c0 = shift[0], c1 = shift[1], c2 = shift[2];
+    const int nx = p.nx, pitch = p.pitch;
+    // low precision: this row's few cells per thread are summed in FP32,
+    // then added to the FP64 accumulators once per row
+    float racc[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) racc[i] = 0.f;
+    for (int x = threadIdx.x; x < nx; x += nc) {
+        const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+        unsigned bits = 0x1fu;
+        if (TEXTURED && WALL != 0) bits = p.wallmask[(size_t)(WALL > 0) * nx * p.ny + (size_t)y * nx + x];
+        Nbr n;
+        if (TEXTURED && ODD && WALL != 0) n = make_nbr(x, y, z, nx, p.ny, pitch);
+        V f[Q];
+#pragma unroll
+        for (int A = 0; A < Q; ++A) {
+            constexpr bool kOdd = ODD;
+            const bool wdir = kOdd && lat_ez(A) != 0 && lat_ez(A) == WALL;
+            V v;
+            if (TEXTURED && wdir) {
+                int slot, idx;
+                switch (A) {
+#define AD(K) case K: aa_address<K, true>(n, WALL, bits, slot, idx); break;
+                    AD(0) AD(1) AD(2) AD(3) AD(4) AD(5) AD(6) AD(7) AD(8) AD(9)
+                    AD(10) AD(11) AD(12) AD(13) AD(14) AD(15) AD(16) AD(17) AD(18)
+#undef AD
+                }
+                v = ld_raw<T>(static_cast<const T *>(p.pop[slot]) + idx);
+            } else {
+                const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
+                v = ld_raw<T>(sb + A * dstride + xs);
+            }
+            f[ODD ? lat_opp(A) : A] = v;
+        }
+        if constexpr (std::is_same<T, double>::value) {
+            const F64Cell c = f64_collide(f, p.omega, G);
+            acc[0] += c.dens;
+            acc[1] += c.jx;
+            acc[2] += c.u0;
+            acc[3] += c.u1;
+            acc[4] += c.u2;
+            const double d0 = c.u0 - c0, d1 = c.u1 - c1, d2 = c.u2 - c2;
+            acc[5] += d0 * d0 + d1 * d1 + d2 * d2;
+            if (CONSTQ) {
+                double s = 0.0, m = 0.0;
+#pragma unroll
+                for (int a = 0; a < Q; ++a) {
+                    s += f[a];
+                    if (lat_ex(a) > 0) m += f[a];
+                    if (lat_ex(a) < 0) m -= f[a];
+                }
+                if (WALL != 0) {  // bounced links arrive with e_x reversed
+                    const int ap = WALL < 0 ? 12 : 11, am = WALL < 0 ? 13 : 14;
+                    if (bits & 2u) m -= 2. * f[ap];
+                    if (bits & 4u) m += 2. * f[am];
+                }
+                acc[6] += s;
+                acc[7] += m;
+            }
+        } else {
+            constexpr float iS = LpStore<T>::kInv;
+            const LpCell c = lp_collide<T>(f, (float)p.omega, (float)G);
+            acc[0] += 1.0;
+            racc[0] += c.drho;
+            racc[1] += c.jx;
+            racc[2] += c.u0;
+            racc[3] += c.u1;
+            racc[4] += c.u2;
+            const float d0 = c.u0 - (float)c0, d1 = c.u1 - (float)c1, d2 = c.u2 - (float)c2;
+            racc[5] += d0 * d0 + d1 * d1 + d2 * d2;
+            if (CONSTQ) {
+                float s = 0.f, m = 0.f;
+#pragma unroll
+                for (int a = 0; a < Q; ++a) {
+                    s += f[a];
+                    if (lat_ex(a)) m += lat_ex(a) > 0 ? f[a] : -f[a];
+                }
+                s *= iS;
+                m *= iS;
+                if (WALL != 0) {  // a bounced link carries -2 e_x (w + d)
+                    const int ap = WALL < 0 ? 12 : 11, am = WALL < 0 ? 13 : 14;
+                    if (bits & 2u) m -= 2.f * (f[ap] * iS + 1.f / 36.f);
+                    if (bits & 4u) m += 2.f * (f[am] * iS + 1.f / 36.f);
+                }
+                acc[6] += 1.0;
+                racc[6] += s;
+                racc[7] += m;
+            }
+        }
+#pragma unroll
+        for (int A = 0; A < Q; ++A) {
+            constexpr bool kOdd = ODD;
+            const bool wdir = kOdd && lat_ez(A) != 0 && lat_ez(A) == WALL;
+            const V v = f[ODD ? A : lat_opp(A)];
+            if (TEXTURED && wdir) {
+                int slot, idx;
+                switch (A) {
+#define AD(K) case K: aa_address<K, true>(n, WALL, bits, slot, idx); break;
+                    AD(0) AD(1) AD(2) AD(3) AD(4) AD(5) AD(6) AD(7) AD(8) AD(9)
+                    AD(10) AD(11) AD(12) AD(13) AD(14) AD(15) AD(16) AD(17) AD(18)
+#undef AD
+                }
+                st_raw<T>(static_cast<T *>(p.pop[slot]) + idx, v);
+            } else {
+                const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
+                st_raw<T>(sb + A * dstride + xs, v);
+            }
+        }
+    }
+    if constexpr (!std::is_same<T, double>::value) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i];
+    }
+}
+
+// ------------------------------------------------------------------ kernel
+// Producer warp: lane A < 19 moves direction A's rows of every row group of
+// the block; lane 0 also arms the stage's full barrier with the byte count.
+template <typename T, bool ODD, bool TEXTURED>
+__device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t, int g0, int n, int lane,
+                                             unsigned char *smem, uint64_t *full, uint64_t *empty, volatile int *abort)
+{
+    const int S = t.stages;
+    const size_t dir_bytes = (size_t)t.k * t.row_bytes, stage_bytes = (size_t)Q * dir_bytes;
+    for (int i = 0; i < n + S; ++i) {
+        const int st = i % S;
+        unsigned char *stage = smem + (size_t)st * stage_bytes;
+        if (i >= S) {  // store group i - S once the consumers have released its stage
+            if (!*abort && !mbar_wait_bounded(empty + st, (uint32_t)((i / S - 1) & 1))) {
+                *abort = 1;
+                atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
+            }
+            const int gi = g0 + i - S, z = gi / t.gpp, y0 = (gi - z * t.gpp) * t.k;
+            const int k = min(t.k, p.ny - y0);
+            const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+            if (lane < Q && !*abort) {
+                const GroupRows g = group_rows<ODD, TEXTURED>(p, lane, y0, z, wall);
+                if (g.bulk) copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, false, nullptr);
+                bulk_commit();
+            }
+        }
+        if (i < n) {  // load group i into the stage
+            const int gi = g0 + i, z = gi / t.gpp, y0 = (gi - z * t.gpp) * t.k;
+            const int k = min(t.k, p.ny - y0);
+            const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+            GroupRows g{};
+            if (lane < Q) g = group_rows<ODD, TEXTURED>(p, lane, y0, z, wall);
+            const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && g.bulk);
+            if (lane < Q) bulk_wait_read_all();  // this lane's store of the stage has read it
+            __syncwarp();
+            if (lane == 0) mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * t.row_bytes));
+            __syncwarp();
+            if (lane < Q && g.bulk && !*abort)
+                copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, true, full + st);
+        }
+    }
+    if (lane < Q) bulk_wait_all();
+}
+
+constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer warp
+
+template <typename T, bool ODD, bool CONSTQ, bool TEXTURED>
+__global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepArgs p, const TmaArgs t)
+{
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    __shared__ int s_abort;
+    const int G_ = t.groups_per_block, S = t.stages;
+    const int g0 = blockIdx.x * G_;
+    const int n = min(g0 + G_, t.ngroups) - g0;
+    if (n <= 0) return;  // block-uniform; empty blocks contribute to no plane
+    const int nc = blockDim.x - 32;  // consumer threads; the last warp produces
+    const size_t dir_bytes = (size_t)t.k * t.row_bytes, stage_bytes = (size_t)Q * dir_bytes;
+    uint64_t *full = reinterpret_cast<uint64_t *>(tma_smem + (size_t)S * stage_bytes);
+    uint64_t *empty = full + S;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, nc / 32);
+        }
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x >= nc) {
+        tma_producer<T, ODD, TEXTURED>(p, t, g0, n, threadIdx.x - nc, tma_smem, full, empty, &s_abort);
+        return;
+    }
+
+    const long long step = *p.step_ctr;
+    const double G = CONSTQ ? p.force[step & 1] : p.gx;
+    const double *shift_now = p.shift + (size_t)(step & 1) * p.nz * 3;
+    const int dstride = t.k * p.pitch;
+    double acc[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) acc[i] = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const int st = i % S, gi = g0 + i;
+        const int z = gi / t.gpp, y0 = (gi - z * t.gpp) * t.k;
+        const int k = min(t.k, p.ny - y0);
+        if (!*(volatile int *)&s_abort && !mbar_wait_bounded(full + st, (uint32_t)((i / S) & 1))) {
+            s_abort = 1;
+            atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
+        }
+        T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
+        const double *sh = shift_now + z * 3;
+        for (int j = 0; j < k; ++j) {
+            T *sbj = sb + (size_t)j * p.pitch;
+            if (z == 0) tma_row<T, ODD, CONSTQ, TEXTURED, -1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+            else if (z == p.nz - 1) tma_row<T, ODD, CONSTQ, TEXTURED, 1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+            else tma_row<T, ODD, CONSTQ, TEXTURED, 0>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+        }
+        fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);
+        if (i + 1 == n || (gi + 1) % t.gpp == 0) {  // this block's last group of plane z
+            const int bfirst = (z * t.gpp) / G_;
+            const int blast = min(((z + 1) * t.gpp - 1) / G_, (t.ngroups - 1) / G_);
+            plane_contribute(p, acc, z, blockIdx.x - bfirst, blast - bfirst + 1, step, G, 0, nc);
+#pragma unroll
+            for (int q = 0; q < NP; ++q) acc[q] = 0.0;
+        }
+    }
+}
+
+template <typename T>
+int tma_set_smem_attr(size_t bytes)
+{
+    const void *ks[] = {
+        (const void *)step_tma_kernel<T, false, false, false>, (const void *)step_tma_kernel<T, false, false, true>,
+        (const void *)step_tma_kernel<T, false, true, false>,  (const void *)step_tma_kernel<T, false, true, true>,
+        (const void *)step_tma_kernel<T, true, false, false>,  (const void *)step_tma_kernel<T, true, false, true>,
+        (const void *)step_tma_kernel<T, true, true, false>,   (const void *)step_tma_kernel<T, true, true, true>};
+    for (const void *k : ks)
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return -1;
+    return 0;
+}
+
+template <typename T>
+int tma_occupancy(int threads, size_t smem)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, false>, threads, smem) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+
+template <typename T>
+void launch_tma(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, bool textured,
+                cudaStream_t s)
+{
+    const bool q = p.const_q != 0;
+#define L(O, C, X) step_tma_kernel<T, O, C, X><<<grid, threads, smem, s>>>(p, t)
+    if (odd) {
+        if (q) { if (textured) L(true, true, true); else L(true, true, false); }
+        else   { if (textured) L(true, false, true); else L(true, false, false); }
+    } else {
+        if (q) { if (textured) L(false, true, true); else L(false, true, false); }
+        else   { if (textured) L(false, false, true); else L(false, false, false); }
+    }
+#undef L
+}
+
+}  // namespace dnslbm

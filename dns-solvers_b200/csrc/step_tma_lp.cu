@@ -1,0 +1,21 @@
+// FP32 / FP16 instantiations of the row-pipelined step (step_tma.cuh).
+#include "step_tma.cuh"
+
+namespace dnslbm {
+
+int tma_prepare_lp(int precision, size_t smem)
+{
+    return precision == 32 ? tma_set_smem_attr<float>(smem) : tma_set_smem_attr<__half>(smem);
+}
+int tma_occupancy_lp(int precision, int threads, size_t smem)
+{
+    return precision == 32 ? tma_occupancy<float>(threads, smem) : tma_occupancy<__half>(threads, smem);
+}
+void launch_tma_lp(int precision, const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd,
+                   bool textured, cudaStream_t s)
+{
+    if (precision == 32) launch_tma<float>(p, t, grid, threads, smem, odd, textured, s);
+    else launch_tma<__half>(p, t, grid, threads, smem, odd, textured, s);
+}
+
+}  // namespace dnslbm

@@ -71,6 +71,8 @@ def lib():
     L.dnslbm_statistics.argtypes = [vp, dp]
     L.dnslbm_moments.argtypes = [vp, dp, dp]
     L.dnslbm_step_timed.argtypes = [vp, ctypes.c_long, dp, dp, dp]
+    L.dnslbm_step_kernel.argtypes = [vp]
+    L.dnslbm_step_kernel.restype = ctypes.c_char_p
     L.dnslbm_bytes_per_cell.argtypes = [vp]
     L.dnslbm_bytes_per_cell.restype = ctypes.c_double
     L.dnslbm_sync.argtypes = [vp]
@@ -186,6 +188,11 @@ class Channel:
         den = np.zeros((x, y, z + 2))
         self._ck(self.L.dnslbm_moments(self.h, _dp(vel), _dp(den)))
         return vel, den
+
+    @property
+    def kernel(self):
+        """Description of the step kernel this context launches."""
+        return self.L.dnslbm_step_kernel(self.h).decode()
 
     @property
     def bytes_per_cell(self):

@@ -134,6 +134,9 @@ int dnslbm_moments(dnslbm_ctx *ctx, double *vel, double *den);
  * CUDA-event times on the context's stream: total, and the summed device
  * time of the two step kernels (even / odd parity launches). */
 int dnslbm_step_timed(dnslbm_ctx *ctx, long nsteps, double *ms_total, double *ms_even, double *ms_odd);
+/* Name of the step kernel this context launches ("row-pipelined bulk-copy"
+ * or "per-thread"), with its launch shape. */
+const char *dnslbm_step_kernel(const dnslbm_ctx *ctx);
 /* Populations bytes moved per fluid cell per step (2*19*storage bytes). */
 double dnslbm_bytes_per_cell(const dnslbm_ctx *ctx);
 /* Block until all work of the context is done. */

@@ -212,3 +212,40 @@ def test_full_size_20_steps_bitexact(oracle_mod, name):
     assert np.isfinite(logs).all()
     oracle_mod.steps(s0, fl, wl.omega, wl.gx, 20)  # in place
     np.testing.assert_array_equal(got, s0)
+
+
+def _with_path(path, fn):
+    old = os.environ.get("DNSLBM_PATH")
+    os.environ["DNSLBM_PATH"] = path
+    try:
+        return fn()
+    finally:
+        if old is None:
+            del os.environ["DNSLBM_PATH"]
+        else:
+            os.environ["DNSLBM_PATH"] = old
+
+
+@pytest.mark.parametrize("prec", [64, 32, 16])
+@pytest.mark.parametrize("tex", ["smooth", "ridges"])
+@pytest.mark.parametrize("const_g", [True, False])
+def test_row_pipelined_and_per_thread_paths_agree(oracle_mod, prec, tex, const_g):
+    """The bulk-copy kernel and the per-thread kernel run the same step:
+    FP64 identical, FP32/FP16 to a few storage roundings."""
+    nx, ny, nz = 44, 18, 9
+    fl = ref_flags(oracle_mod, tex, nx, ny, nz)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 13)
+
+    def run():
+        ch = gpu_run(s0, fl, 1.7, 7, gx=2e-5, ubulk=0.07, const_g=const_g, precision=prec)
+        return ch.kernel, ch.store_state(), ch.logs()
+
+    kt, st_t, lg_t = run()
+    ks, st_s, lg_s = _with_path("scalar", run)
+    assert "bulk-copy" in kt and "per-thread" in ks
+    if prec == 64 and const_g:
+        np.testing.assert_array_equal(st_t, st_s)
+    else:
+        tol = {64: 1e-13, 32: 1e-6, 16: 2e-3}[prec]
+        np.testing.assert_allclose(st_t, st_s, rtol=0, atol=tol)
+    np.testing.assert_allclose(lg_t, lg_s, rtol=1e-5 if prec < 64 else 1e-11, atol=1e-12)

@@ -2,7 +2,7 @@
 
 Each result states its error against the FP64 oracle (the CPU restatement,
 which the FP64 GPU kernel matches bit for bit).  Bounds asserted here:
-  FP32: populations within 2e-7 absolute after 200 laminar steps; the mean
+  FP32: populations within 5e-7 absolute after 200 laminar steps; the mean
         velocity profile within 5e-5 relative (measured 1.03e-5 on a B200: the
         per-step force increment w*3*g ~ 1e-7 is ~1% of an FP32 ulp of the
         stored deviations, so its rounding accumulates).
@@ -17,7 +17,7 @@ import inputs
 
 pytestmark = pytest.mark.gpu
 
-BOUNDS = {32: (2e-7, 5e-5), 16: (2e-4, 5e-3)}
+BOUNDS = {32: (5e-7, 5e-5), 16: (2e-4, 5e-3)}
 
 
 def run(prec, s0, fl, omega, gx, steps):
