@@ -218,10 +218,11 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         const size_t smem = (size_t)stages * smem_stage + 16 * (size_t)stages;  // + full/empty mbarriers
         const bool fits = stages >= 2 && smem <= (size_t)maxsmem && nsm > 0;
         if (fits && !(path && !strcmp(path, "scalar"))) {
-            // consumer threads: about 2 cells each along the row, at most 352
-            int cpt = (c->nx + 319) / 320;
-            int consumers = ((c->nx + cpt - 1) / cpt + 31) / 32 * 32;
-            if (c->deck.precision == 16) consumers = std::min(consumers, 128);  // two blocks per SM
+            // consumer threads (measured on a B200, 628-wide rows): about 2
+            // cells each for FP64 (at most 320), 3 for FP32 (at most 192), 5
+            // for FP16 (at most 128, so two blocks share an SM)
+            const int cap = c->deck.precision == 64 ? 320 : (c->deck.precision == 32 ? 192 : 128);
+            int consumers = std::min(cap, (c->nx + 31) / 32 * 32);
             if (const char *e = getenv("DNSLBM_THREADS")) consumers = atoi(e) / 32 * 32;
             if (consumers > 352) consumers = 352;
             if (consumers < 32) consumers = 32;

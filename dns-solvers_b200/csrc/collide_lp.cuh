@@ -46,6 +46,49 @@ struct LpCell {
     float drho, jx, u0, u1, u2;  // drho = rho - 1, jx unscaled
 };
 
+// e_a . u with every 0/+-1 factor resolved at compile time (a multiplication
+// by a constant zero is not foldable under IEEE rules).
+template <int A>
+__device__ __forceinline__ float lp_eu(float u0, float u1, float u2)
+{
+    constexpr int ex = lat_ex(A), ey = lat_ey(A), ez = lat_ez(A);
+    float s = 0.f;
+    bool first = true;
+    if (ex != 0) { s = ex > 0 ? u0 : -u0; first = false; }
+    if (ey != 0) { s = first ? (ey > 0 ? u1 : -u1) : (ey > 0 ? s + u1 : s - u1); first = false; }
+    if (ez != 0) { s = first ? (ez > 0 ? u2 : -u2) : (ez > 0 ? s + u2 : s - u2); }
+    return s;
+}
+
+// Per-cell constants of the pair update, per weight class (1/18, 1/36).
+struct LpConst {
+    float dr, Srho, usq15, om1;
+    float wom[2], a0[2], b_eu[2], b_ex[2], a_eu[2];
+};
+
+// Pair (a, opp a): A = w (omega (dr + S rho t) + S G (9 e_x e.u - 3 u_x)),
+// B = w (3 omega S rho e.u + 3 S G e_x), t = 4.5 (e.u)^2 - 1.5 u.u.
+template <int K>
+__device__ __forceinline__ void lp_pair(float (&r)[Q], const LpConst &k, float u0, float u1, float u2)
+{
+    constexpr int a = pair_dir(K), b = lat_opp(pair_dir(K));
+    constexpr int cls = lat_wclass(a) - 1;
+    constexpr int ex = lat_ex(a);
+    const float eu = lp_eu<a>(u0, u1, u2);
+    const float t = fmaf(4.5f * eu, eu, -k.usq15);
+    const float X = fmaf(k.Srho, t, k.dr);
+    float A, B;
+    if (ex == 0) {
+        A = fmaf(k.wom[cls], X, k.a0[cls]);
+        B = k.b_eu[cls] * eu;
+    } else {
+        A = fmaf(k.wom[cls], X, fmaf(ex > 0 ? k.a_eu[cls] : -k.a_eu[cls], eu, k.a0[cls]));
+        B = fmaf(k.b_eu[cls], eu, ex > 0 ? k.b_ex[cls] : -k.b_ex[cls]);
+    }
+    r[a] = fmaf(k.om1, r[a], A + B);
+    r[b] = fmaf(k.om1, r[b], A - B);
+}
+
 // In place on raw values r[19] of one storage type with scale S.
 template <typename T>
 __device__ __forceinline__ LpCell lp_collide(float (&r)[Q], float omega, float G)
@@ -77,24 +120,32 @@ __device__ __forceinline__ LpCell lp_collide(float (&r)[Q], float omega, float G
     c.u0 = jx * inv;
     c.u1 = jy * inv;
     c.u2 = jz * inv;
-    const float usq15 = 1.5f * (c.u0 * c.u0 + c.u1 * c.u1 + c.u2 * c.u2);
-    const float Srho = S * rho, SG = S * G, om1 = 1.f - omega;
-    // rest direction
-    {
-        constexpr float w = 1.f / 3.f;
-        r[0] = fmaf(om1, r[0], w * (omega * fmaf(Srho, -usq15, dr) - 3.f * SG * c.u0));
-    }
+    LpConst k;
+    k.dr = dr;
+    k.Srho = S * rho;
+    k.usq15 = 1.5f * (c.u0 * c.u0 + c.u1 * c.u1 + c.u2 * c.u2);
+    k.om1 = 1.f - omega;
+    const float SG = S * G;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        const int a = pair_dir(k), b = lat_opp(a);
-        const float w = lat_wf(a);
-        const float eu = (float)lat_ex(a) * c.u0 + (float)lat_ey(a) * c.u1 + (float)lat_ez(a) * c.u2;
-        const float t = fmaf(4.5f * eu, eu, -usq15);
-        const float A = w * (omega * fmaf(Srho, t, dr) + SG * fmaf(9.f * (float)lat_ex(a), eu, -3.f * c.u0));
-        const float B = w * (omega * 3.f * Srho * eu + 3.f * SG * (float)lat_ex(a));
-        r[a] = fmaf(om1, r[a], A + B);
-        r[b] = fmaf(om1, r[b], A - B);
+    for (int q = 0; q < 2; ++q) {
+        const float w = q == 0 ? 1.f / 18.f : 1.f / 36.f;
+        k.wom[q] = w * omega;
+        k.a0[q] = -3.f * w * SG * c.u0;
+        k.a_eu[q] = 9.f * w * SG;
+        k.b_eu[q] = 3.f * w * omega * k.Srho;
+        k.b_ex[q] = 3.f * w * SG;
     }
+    // rest direction
+    r[0] = fmaf(k.om1, r[0], (1.f / 3.f) * fmaf(omega, fmaf(k.Srho, -k.usq15, dr), -3.f * SG * c.u0));
+    lp_pair<0>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<1>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<2>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<3>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<4>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<5>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<6>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<7>(r, k, c.u0, c.u1, c.u2);
+    lp_pair<8>(r, k, c.u0, c.u1, c.u2);
     return c;
 }
 
