@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch shapes")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU-baseline sample")
     return ap.parse_args()
 
@@ -240,6 +241,7 @@ def run_ours(args):
 
     ch = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, ubulk=wl.ubulk, gx=wl.gx, force_mode=dnslbm.CONST_G,
                         precision=args.precision, device=dev)
+    tune = None if args.no_autotune else ch.autotune()
     ch.set_flags(flags)
     ch.load_state(s0)
     ch.step_timed(args.warmup)
@@ -265,7 +267,7 @@ def run_ours(args):
     traffic = ncu_traffic(f"{wl.name}:f{args.precision}")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": f"{peak_src} (MEASURED_PEAKS.json)",
-            "kernel": kname, "kernel_config": kdesc, "launch_ms": round(launch_s * 1e3, 4),
+            "kernel": kname, "kernel_config": kdesc, "autotune": tune, "launch_ms": round(launch_s * 1e3, 4),
             "whole_step_frac": round(bpc * cells / (tmax / args.steps / 1e3) / 1e9 / peak, 4),
             "algorithmic_bytes_per_launch": bpc * cells, "bytes_per_cell": bpc}
 
@@ -277,6 +279,7 @@ def run_ours(args):
         for prec in (32, 16):
             c2 = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, ubulk=wl.ubulk, gx=wl.gx,
                                 force_mode=dnslbm.CONST_G, precision=prec, device=dev)
+            tune2 = None if args.no_autotune else c2.autotune()
             c2.set_flags(flags)
             c2.load_state(s0)
             c2.step_timed(args.warmup)
@@ -294,7 +297,9 @@ def run_ours(args):
                 "ms_per_step": round(t2 / args.steps, 4), "speedup_vs_f64": round(tot / t2, 3),
                 "roofline": {"bound": "hbm", "achieved": round(ach2, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(ach2 / peak, 4), "bytes_per_cell": b2,
-                             "traffic": ncu_traffic(f"{wl.name}:f{prec}")},
+                             "whole_step_frac": round(b2 * cells / (t2 / args.steps / 1e3) / 1e9 / peak, 4),
+                             "traffic": ncu_traffic(f"{wl.name}:f{prec}"), "kernel_config": c2.kernel,
+                             "autotune": tune2},
                 "error_vs_f64": {
                     "after_steps": done,
                     "mean_u_profile_max_rel": float(np.max(np.abs(um - um_ref)) / np.max(np.abs(um_ref))),

@@ -141,6 +141,54 @@ static void free_all(dnslbm_ctx *c)
 
 extern "C" const char *dnslbm_last_error(const dnslbm_ctx *c) { return c ? c->err : g_create_err; }
 
+// Configure the row-pipelined step with k rows per stage group, `stages`
+// groups in flight and `consumers` compute threads (+ one producer warp);
+// bps > 0 caps the blocks per SM.  Returns 0 when the configuration runs on
+// this device (and selects it), -1 otherwise (the previous choice stays).
+static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bps)
+{
+    const int row_bytes = c->pitch * (int)c->esize;
+    k = std::max(1, std::min(k, c->ny));
+    consumers = std::max(32, std::min(352, consumers / 32 * 32));
+    const size_t smem_stage = (size_t)Q * row_bytes * k;
+    int maxsmem = 0, nsm = 0;
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->deck.device);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->deck.device);
+    const size_t smem = (size_t)stages * smem_stage + 16 * (size_t)stages;  // + full/empty mbarriers
+    if (stages < 2 || smem > (size_t)maxsmem || nsm <= 0) return -1;
+    const int threads = consumers + 32;
+    const int prep = c->deck.precision == 64 ? tma_prepare_f64(smem) : tma_prepare_lp(c->deck.precision, smem);
+    int occ = prep ? 0
+                   : (c->deck.precision == 64 ? tma_occupancy_f64(threads, smem)
+                                              : tma_occupancy_lp(c->deck.precision, threads, smem));
+    cudaGetLastError();  // a failed query only rules the configuration out
+    if (bps > 0) occ = std::min(occ, bps);
+    if (occ < 1) return -1;
+    const int gpp = (c->ny + k - 1) / k, ngroups = gpp * c->nz;
+    const int target = occ * nsm;
+    const int GB = (ngroups + target - 1) / target;
+    c->use_tma = 1;
+    c->tma_threads = threads;
+    c->tma_smem = smem;
+    c->tma_grid = (ngroups + GB - 1) / GB;
+    c->tma = TmaArgs{ngroups, GB, stages, row_bytes, k, gpp};
+    return 0;
+}
+
+static void describe_kernel(dnslbm_ctx *c)
+{
+    if (c->use_tma)
+        snprintf(c->kernel_desc, sizeof c->kernel_desc,
+                 "step_tma_kernel<fp%d> row-pipelined bulk-copy: %d blocks x %d threads, %d groups of %d rows/block, "
+                 "%d stages, %zu B smem",
+                 c->deck.precision, c->tma_grid, c->tma_threads, c->tma.groups_per_block, c->tma.k, c->tma.stages,
+                 c->tma_smem);
+    else
+        snprintf(c->kernel_desc, sizeof c->kernel_desc, "%s per-thread: grid %ux%ux%u x %u threads",
+                 c->deck.precision == 64 ? "step_f64_kernel" : "step_lp_kernel", c->grid.x, c->grid.y, c->grid.z,
+                 c->block.x);
+}
+
 extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
 {
     dnslbm_ctx *c = nullptr;
@@ -196,66 +244,32 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     c->grid = dim3((c->nx + bx - 1) / bx, (c->ny + c->rows - 1) / c->rows, c->nz);
     c->slots = (int)(c->grid.x * c->grid.y);
     {
-        // row-pipelined step: whole rows through shared memory, `stages`
-        // rows in flight per block; used when two stages fit
+        // Row-pipelined step.  A stage holds a group of k consecutive rows of
+        // one plane for all 19 directions.  Defaults measured on a B200
+        // (628-wide rows): two stages of about 48 KB (FP16) to 96 KB
+        // (FP32/FP64) per block; consumer threads about 2 cells each for FP64
+        // (at most 320), 3 for FP32 (at most 192), 5 for FP16 (at most 128, so
+        // two blocks share an SM).  dnslbm_autotune replaces them by measured
+        // choices; the DNSLBM_* environment variables override them.
         const char *path = getenv("DNSLBM_PATH");
         const int row_bytes = c->pitch * (int)c->esize;
-        // A stage holds a group of k consecutive rows of one plane for all 19
-        // directions.  Defaults measured on a B200 (628-wide rows): two
-        // stages of about 48 KB (FP16) to 96 KB (FP32/FP64) per block, whole
-        // rows per consumer thread pair; FP16 runs two blocks per SM.
         const size_t stage_target = c->deck.precision == 16 ? 49152 : 98304;
         int k = 1;
         while (k < 8 && k * 2 <= c->ny && (size_t)Q * row_bytes * k * 2 <= stage_target) k *= 2;
         if (const char *e = getenv("DNSLBM_GROUP_ROWS")) k = std::max(1, std::min(atoi(e), c->ny));
-        const size_t smem_stage = (size_t)Q * row_bytes * k;
-        int maxsmem = 0, nsm = 0;
-        cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, deck->device);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, deck->device);
         int stages = 2;
         if (const char *e = getenv("DNSLBM_STAGES")) stages = atoi(e);
-        while (stages > 2 && (size_t)stages * smem_stage + 16 * (size_t)stages > (size_t)maxsmem) --stages;
-        const size_t smem = (size_t)stages * smem_stage + 16 * (size_t)stages;  // + full/empty mbarriers
-        const bool fits = stages >= 2 && smem <= (size_t)maxsmem && nsm > 0;
-        if (fits && !(path && !strcmp(path, "scalar"))) {
-            // consumer threads (measured on a B200, 628-wide rows): about 2
-            // cells each for FP64 (at most 320), 3 for FP32 (at most 192), 5
-            // for FP16 (at most 128, so two blocks share an SM)
-            const int cap = c->deck.precision == 64 ? 320 : (c->deck.precision == 32 ? 192 : 128);
-            int consumers = std::min(cap, (c->nx + 31) / 32 * 32);
-            if (const char *e = getenv("DNSLBM_THREADS")) consumers = atoi(e) / 32 * 32;
-            if (consumers > 352) consumers = 352;
-            if (consumers < 32) consumers = 32;
-            const int threads = consumers + 32;
-            int prep = c->deck.precision == 64 ? tma_prepare_f64(smem) : tma_prepare_lp(c->deck.precision, smem);
-            int occ = prep ? 0
-                           : (c->deck.precision == 64 ? tma_occupancy_f64(threads, smem)
-                                                      : tma_occupancy_lp(c->deck.precision, threads, smem));
-            if (const char *e = getenv("DNSLBM_BLOCKS_PER_SM")) occ = std::min(occ, atoi(e));
-            if (occ >= 1) {
-                const int gpp = (c->ny + k - 1) / k, ngroups = gpp * c->nz;
-                const int target = occ * nsm;
-                const int GB = (ngroups + target - 1) / target;
-                c->use_tma = 1;
-                c->tma_threads = threads;
-                c->tma_smem = smem;
-                c->tma_grid = (ngroups + GB - 1) / GB;
-                c->tma = TmaArgs{ngroups, GB, stages, row_bytes, k, gpp};
-                c->slots = std::max(c->slots, (gpp + GB - 1) / GB + 1);
-            }
-        }
-        cudaGetLastError();  // an attribute query that failed only selects the scalar path
+        const int cap = c->deck.precision == 64 ? 320 : (c->deck.precision == 32 ? 192 : 128);
+        int consumers = std::min(cap, (c->nx + 31) / 32 * 32);
+        if (const char *e = getenv("DNSLBM_THREADS")) consumers = atoi(e) / 32 * 32;
+        int bps = 0;
+        if (const char *e = getenv("DNSLBM_BLOCKS_PER_SM")) bps = atoi(e);
+        if (!(path && !strcmp(path, "scalar"))) tma_configure(c, k, stages, consumers, bps);
+        describe_kernel(c);
     }
-    if (c->use_tma)
-        snprintf(c->kernel_desc, sizeof c->kernel_desc,
-                 "step_tma_kernel<fp%d> row-pipelined bulk-copy: %d blocks x %d threads, %d groups of %d rows/block, "
-                 "%d stages, %zu B smem",
-                 c->deck.precision, c->tma_grid, c->tma_threads, c->tma.groups_per_block, c->tma.k, c->tma.stages,
-                 c->tma_smem);
-    else
-        snprintf(c->kernel_desc, sizeof c->kernel_desc, "%s per-thread: grid %ux%ux%u x %u threads",
-                 c->deck.precision == 64 ? "step_f64_kernel" : "step_lp_kernel", c->grid.x, c->grid.y, c->grid.z,
-                 c->block.x);
+    // partial-sum slots: enough for the per-thread kernels and for any row
+    // group split the tuner may choose
+    c->slots = std::max(c->slots, c->ny + 1);
     const size_t nblocks = (size_t)c->nz * c->slots;
 
     struct Alloc { void **p; size_t bytes; };
@@ -666,4 +680,89 @@ extern "C" void *dnslbm_host_alloc(size_t bytes)
 extern "C" void dnslbm_host_free(void *p)
 {
     if (p) cudaFreeHost(p);
+}
+
+// ---------------------------------------------------------------- autotuner
+struct TmaChoice {
+    int use_tma, threads, grid;
+    size_t smem;
+    TmaArgs t;
+};
+
+static TmaChoice save_choice(const dnslbm_ctx *c) { return {c->use_tma, c->tma_threads, c->tma_grid, c->tma_smem, c->tma}; }
+static void load_choice(dnslbm_ctx *c, const TmaChoice &k)
+{
+    c->use_tma = k.use_tma;
+    c->tma_threads = k.threads;
+    c->tma_grid = k.grid;
+    c->tma_smem = k.smem;
+    c->tma = k.t;
+}
+
+// device time per step of the current launch shape, on a rest state
+static int time_choice(dnslbm_ctx *c, int steps, double *ms)
+{
+    int rc = reset_counters(c);
+    if (rc) return rc;
+    launch_io(c->deck.precision, 2, io_args(c), 0, 0, nullptr, nullptr, c->stream);
+    CK(cudaGetLastError());
+    if ((rc = initial_reduce(c))) return rc;
+    double e = 0, o = 0;
+    if ((rc = launch_steps(c, 2, true, &e, &o))) return rc;
+    e = o = 0;
+    if ((rc = launch_steps(c, steps, true, &e, &o))) return rc;
+    if ((rc = check_status(c))) return rc;
+    *ms = (e + o) / steps;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t report_len)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (c->have_state) return fail(c, DNSLBM_ERR_STATE, "autotune runs before a state is loaded (it steps a rest state)");
+    if (steps < 2) steps = 2;
+    CK(cudaSetDevice(c->deck.device));
+    int ncand = 0;
+    double best_ms = 1e30;
+    TmaChoice best = save_choice(c);
+    int rc;
+    // the per-thread kernel
+    {
+        c->use_tma = 0;
+        double ms;
+        if ((rc = time_choice(c, steps, &ms))) return rc;
+        ++ncand;
+        if (ms < best_ms) best_ms = ms, best = save_choice(c);
+    }
+    // row-pipelined: group rows x stages at the default consumer count, then
+    // the consumer count for the best pair
+    const int cap = c->deck.precision == 64 ? 320 : (c->deck.precision == 32 ? 192 : 128);
+    const int cons0 = std::min(cap, (c->nx + 31) / 32 * 32);
+    int bk = -1, bs = -1;
+    for (int k : {1, 2, 4, 8})
+        for (int st : {2, 3, 4}) {
+            if (k > c->ny || tma_configure(c, k, st, cons0, 0)) continue;
+            double ms;
+            if ((rc = time_choice(c, steps, &ms))) return rc;
+            ++ncand;
+            if (ms < best_ms) best_ms = ms, best = save_choice(c), bk = k, bs = st;
+        }
+    if (bk > 0)
+        for (int cons = 64; cons <= 352 && cons <= (c->nx + 31) / 32 * 32 + 32; cons += 32) {
+            if (cons == cons0 || tma_configure(c, bk, bs, cons, 0)) continue;
+            double ms;
+            if ((rc = time_choice(c, steps, &ms))) return rc;
+            ++ncand;
+            if (ms < best_ms) best_ms = ms, best = save_choice(c);
+        }
+    load_choice(c, best);
+    describe_kernel(c);
+    // leave the context as created: no state, counters clear
+    if ((rc = reset_counters(c))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_state = 0;
+    if (report && report_len)
+        snprintf(report, report_len, "%s: %.4f ms/step (best of %d launch shapes, %d steps each)", c->kernel_desc,
+                 best_ms, ncand, steps);
+    return DNSLBM_OK;
 }

@@ -71,6 +71,7 @@ def lib():
     L.dnslbm_statistics.argtypes = [vp, dp]
     L.dnslbm_moments.argtypes = [vp, dp, dp]
     L.dnslbm_step_timed.argtypes = [vp, ctypes.c_long, dp, dp, dp]
+    L.dnslbm_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     L.dnslbm_step_kernel.argtypes = [vp]
     L.dnslbm_step_kernel.restype = ctypes.c_char_p
     L.dnslbm_bytes_per_cell.argtypes = [vp]
@@ -188,6 +189,13 @@ class Channel:
         den = np.zeros((x, y, z + 2))
         self._ck(self.L.dnslbm_moments(self.h, _dp(vel), _dp(den)))
         return vel, den
+
+    def autotune(self, steps=6):
+        """Time the candidate launch shapes on this grid and keep the fastest
+        (call before loading a state).  Returns the tuner's one-line report."""
+        buf = ctypes.create_string_buffer(512)
+        self._ck(self.L.dnslbm_autotune(self.h, steps, buf, len(buf)))
+        return buf.value.decode()
 
     @property
     def kernel(self):

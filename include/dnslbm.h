@@ -134,6 +134,16 @@ int dnslbm_moments(dnslbm_ctx *ctx, double *vel, double *den);
  * CUDA-event times on the context's stream: total, and the summed device
  * time of the two step kernels (even / odd parity launches). */
 int dnslbm_step_timed(dnslbm_ctx *ctx, long nsteps, double *ms_total, double *ms_even, double *ms_odd);
+/* Autotuner: choose the step kernel's launch shape (per-thread kernel, or the
+ * row-pipelined kernel's rows per stage group, stages in flight and consumer
+ * warps) by timing each candidate for `steps` steps on this context's own grid
+ * and precision, and keep the fastest.  Call it after dnslbm_create and before
+ * a state is set: it steps a rest state and leaves the context without one.
+ * report (may be NULL) receives the choice and its time.  No counterpart in
+ * the reference, whose loop tiling is the compile-time constant cs
+ * (definitions.h:117). */
+int dnslbm_autotune(dnslbm_ctx *ctx, int steps, char *report, size_t report_len);
+
 /* Name of the step kernel this context launches ("row-pipelined bulk-copy"
  * or "per-thread"), with its launch shape. */
 const char *dnslbm_step_kernel(const dnslbm_ctx *ctx);

@@ -249,3 +249,28 @@ def test_row_pipelined_and_per_thread_paths_agree(oracle_mod, prec, tex, const_g
         tol = {64: 1e-13, 32: 1e-6, 16: 2e-3}[prec]
         np.testing.assert_allclose(st_t, st_s, rtol=0, atol=tol)
     np.testing.assert_allclose(lg_t, lg_s, rtol=1e-5 if prec < 64 else 1e-11, atol=1e-12)
+
+
+@pytest.mark.parametrize("prec", [64, 16])
+def test_autotuned_kernel_is_exact_and_tuning_needs_no_state(oracle_mod, prec):
+    """dnslbm_autotune picks a launch shape by timing; whatever it picks
+    computes the same step (FP64 bit-exact), and it refuses to run once a
+    state is loaded (it would overwrite it)."""
+    nx, ny, nz = 40, 20, 10
+    fl = inputs.flags_longitudinal(nx, ny, nz, 3, 3)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 17)
+    ch = dnslbm.Channel(nx, ny, nz, 1.8, gx=2e-5, force_mode=dnslbm.CONST_G, precision=prec)
+    report = ch.autotune(steps=3)
+    assert "ms/step" in report and ch.kernel in report
+    ch.set_flags(fl)
+    ch.load_state(s0)
+    ch.step(9)
+    ref = s0.copy()
+    oracle_mod.run(ref, fl, 1.8, gx=2e-5, const_g=True, nsteps=9)
+    if prec == 64:
+        np.testing.assert_array_equal(ch.store_state(), ref)
+    else:
+        np.testing.assert_allclose(ch.store_state(), ref, rtol=0, atol=2e-4)
+    with pytest.raises(dnslbm.DnsLbmError) as e:
+        ch.autotune()
+    assert e.value.code == dnslbm.ERR_STATE
