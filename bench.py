@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch shapes")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 24-channel batched FP32 measurement")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU-baseline sample")
     return ap.parse_args()
 
@@ -226,6 +227,64 @@ def timed_run(ch, steps, warmup):
     return ch.step_timed(steps)
 
 
+def batched_report(args, dev):
+    """24 independent FP32 channels (half-heights 20/32/48/64, seeded walls
+    and Re_tau in [120, 180]) advanced by one launch per step with the time
+    loop replayed from a CUDA graph, against the same channels stepped one at
+    a time, each alone on the GPU (both arms autotuned unless --no-autotune).
+    Initial fields: one turbulent-like field per half-height, shared by the
+    channels of that height, with solid cells set to rest."""
+    import dnslbm
+    import inputs
+    chans = inputs.batch_channels(24, seed=0)
+    fields = {}
+    for w in chans:
+        if w.nz not in fields:
+            fields[w.nz] = inputs.turbulent_state(w.nx, w.ny, w.nz, w.ubulk, 0.1, w.nz)
+
+    def mode(w):
+        return dnslbm.BC_GENERAL if inputs.needs_general(w) else dnslbm.BC_REFERENCE
+
+    def start(c, w):
+        fl = inputs.make_flags(w)
+        c.set_flags(fl)
+        c.load_state(inputs.rest_solids(fields[w.nz], fl) if inputs.needs_general(w) else fields[w.nz])
+
+    decks = [dnslbm.deck(w.nx, w.ny, w.nz, w.omega, ubulk=w.ubulk, gx=w.gx, precision=32, bc_mode=mode(w),
+                         device=dev) for w in chans]
+    cells = sum(w.cells for w in chans)
+    warm = max(args.warmup, 3)
+    with dnslbm.Batch(decks) as b:
+        tune = None if args.no_autotune else b.autotune(8)
+        for c, w in zip(b.channels, chans):
+            start(c, w)
+        b.step_timed(warm)
+        ms_b = b.step_timed(args.steps)
+        kdesc = b.kernel
+        bpc = b.channels[0].bytes_per_cell
+    ms_alone = 0.0
+    for w in chans:
+        with dnslbm.Channel(w.nx, w.ny, w.nz, w.omega, ubulk=w.ubulk, gx=w.gx, precision=32, bc_mode=mode(w),
+                            device=dev) as c:
+            if not args.no_autotune:
+                c.autotune()
+            start(c, w)
+            c.step_timed(warm)
+            ms_alone += c.step_timed(args.steps)[0]
+    peak, _ = hbm_peak()
+    return {"workload": "24 channels, h in {20, 32, 48, 64}, (2 pi h) x (2h + 2) x (pi h), seeded walls "
+                        "(smooth / longitudinal grooves / transverse grooves / triangular riblets), Re_tau in "
+                        "[120, 180]",
+            "channels": [w.name for w in chans], "cells": cells, "dtype": "f32", "steps": args.steps,
+            "value": round(cells * args.steps / (ms_b / 1e3) / 1e6, 1), "unit": "MLUPS",
+            "ms_per_step": round(ms_b / args.steps, 4),
+            "one_at_a_time": {"value": round(cells * args.steps / (ms_alone / 1e3) / 1e6, 1), "unit": "MLUPS",
+                              "ms_per_step": round(ms_alone / args.steps, 4)},
+            "speedup_vs_one_at_a_time": round(ms_alone / ms_b, 3),
+            "whole_step_frac_of_hbm": round(bpc * cells / (ms_b / args.steps / 1e3) / 1e9 / peak, 4),
+            "kernel_config": kdesc, "autotune": tune}
+
+
 def run_ours(args):
     import numpy as np
 
@@ -311,6 +370,13 @@ def run_ours(args):
             c2.close()
         del ref_vel
 
+    batched = None
+    if not args.no_batched:
+        try:
+            batched = batched_report(args, dev)
+        except Exception as e:  # reported, never fatal
+            batched = {"error": str(e)[:300]}
+
     e2e = None
     if not args.no_e2e:
         state_bytes = s0.nbytes
@@ -353,7 +419,7 @@ def run_ours(args):
                            "walls": wl.texture, "force": f"constant g={wl.gx:.3e}", "omega": wl.omega,
                            "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU",
                            "l2": f"state {cells * 19 * args.precision / 8 / 1e9:.2f} GB vs 126 MB L2, no flush"},
-                "roofline": roof, "variants": variants, "e2e": e2e, "cpu_baseline": cb,
+                "roofline": roof, "variants": variants, "batched": batched, "e2e": e2e, "cpu_baseline": cb,
                 "gpu_launches": args.steps, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     ch.close()

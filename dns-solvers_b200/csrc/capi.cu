@@ -11,26 +11,32 @@
 
 #include "../../include/dnslbm.h"
 #include "step_common.cuh"
+#include "step_tma.cuh"
 
 namespace dnslbm {
-void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, bool textured, cudaStream_t s);
+void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex, cudaStream_t s);
 void launch_reduce_f64(const StepArgs &p, dim3 grid, dim3 block, cudaStream_t s);
-void launch_step_lp(int precision, const StepArgs &p, dim3 grid, dim3 block, bool odd, bool textured, cudaStream_t s);
+void launch_step_lp(int precision, const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex, cudaStream_t s);
 void launch_reduce_lp(int precision, const StepArgs &p, dim3 grid, dim3 block, cudaStream_t s);
 void launch_io(int precision, int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s);
 void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int rows, int pass, const double *mean,
                   double *partials, double *plane_out, cudaStream_t s);
-struct TmaArgs {
-    int ngroups, groups_per_block, stages, row_bytes, k, gpp;
-};
 int tma_prepare_f64(size_t smem);
 int tma_occupancy_f64(int threads, size_t smem);
-void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, bool textured,
+void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
                     cudaStream_t s);
 int tma_prepare_lp(int precision, size_t smem);
 int tma_occupancy_lp(int precision, int threads, size_t smem);
 void launch_tma_lp(int precision, const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd,
-                   bool textured, cudaStream_t s);
+                   int tex, cudaStream_t s);
+int tma_batch_prepare_f64(size_t smem);
+int tma_batch_occupancy_f64(int threads, size_t smem);
+void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem, bool odd,
+                          cudaStream_t s);
+int tma_batch_prepare_lp(int precision, size_t smem);
+int tma_batch_occupancy_lp(int precision, int threads, size_t smem);
+void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem,
+                         bool odd, cudaStream_t s);
 }  // namespace dnslbm
 
 using namespace dnslbm;
@@ -42,7 +48,11 @@ struct dnslbm_ctx {
     size_t ncell, pstride, esize;
     void *popmem = nullptr;
     uint8_t *wallmask = nullptr;
-    int textured = 0;
+    int textured = 0;  // 0 smooth walls, 1 textured walls, 2 solids inside the flow
+    int *band_of = nullptr;      // [nz] mask block of a plane next to a solid, -1: none
+    unsigned *links = nullptr;   // [nband][ny][nx] per-cell link masks
+    size_t links_bytes = 0;
+    int nband = 0;
     double *force = nullptr, *shift = nullptr, *partials = nullptr, *plane_sums = nullptr, *logs = nullptr;
     long long *step_ctr = nullptr, *status = nullptr;
     unsigned *plane_ctr = nullptr, *total_ctr = nullptr;
@@ -109,6 +119,8 @@ static StepArgs step_args(const dnslbm_ctx *c)
     p.logs = c->logs;
     p.log_cap = c->deck.log_capacity;
     p.status = c->status;
+    p.band_of = c->band_of;
+    p.links = c->links;
     return p;
 }
 
@@ -123,13 +135,15 @@ static IoArgs io_args(const dnslbm_ctx *c)
     p.wallmask = c->wallmask;
     p.textured = c->textured;
     p.odd = c->odd;
+    p.band_of = c->band_of;
+    p.links = c->links;
     return p;
 }
 
 static void free_all(dnslbm_ctx *c)
 {
     void *ptrs[] = {c->popmem, c->wallmask, c->force, c->shift, c->partials, c->plane_sums, c->logs, c->step_ctr,
-                    c->status, c->plane_ctr, c->total_ctr, c->staging, c->stat_partials, c->stat_planes, c->stat_mean};
+                    c->status, c->plane_ctr, c->total_ctr, c->staging, c->stat_partials, c->stat_planes, c->stat_mean, c->band_of, c->links};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : c->ev)
@@ -292,6 +306,7 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         {(void **)&c->stat_partials, nblocks * 5 * sizeof(double)},
         {(void **)&c->stat_planes, (size_t)c->nz * 5 * sizeof(double)},
         {(void **)&c->stat_mean, (size_t)c->nz * 4 * sizeof(double)},
+        {(void **)&c->band_of, (size_t)c->nz * sizeof(int)},
     };
     for (auto &a : al) {
         cudaError_t e = cudaMalloc(a.p, a.bytes);
@@ -310,9 +325,10 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
             fail(c, DNSLBM_ERR_CUDA, "cannot create event");
             return bail(DNSLBM_ERR_CUDA);
         }
-    // default flags: smooth no-slip walls (solid_init.c)
+    // default flags: smooth no-slip walls (solid_init.c), no solid inside
     std::vector<uint8_t> m((size_t)2 * c->nx * c->ny, 0x1f);
     if (cudaMemcpy(c->wallmask, m.data(), m.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(c->band_of, 0xff, (size_t)c->nz * sizeof(int)) != cudaSuccess ||
         cudaDeviceSynchronize() != cudaSuccess) {
         fail(c, DNSLBM_ERR_CUDA, "initialisation failed: %s", cudaGetErrorString(cudaGetLastError()));
         return bail(DNSLBM_ERR_CUDA);
@@ -331,13 +347,25 @@ extern "C" void dnslbm_destroy(dnslbm_ctx *c)
     delete c;
 }
 
+static int initial_reduce(dnslbm_ctx *c);
+
 // wall-link bits from the wall-plane flags (xcomputations.c:368-375): the
 // link from fluid cell P toward wall cell T bounces back iff s(T) == -1 and
 // s(P's own wall cell) == -1; otherwise it reflects specularly.
+//
+// Boundary mode DNSLBM_BC_GENERAL also takes solid cells (-1) inside the
+// flow.  Every plane within one plane of such a cell gets per-cell link
+// masks (cell_links): a link from a fluid cell bounces back when its target
+// is solid, when both wall cells of the wall rule are no-slip, or when the
+// specular reflection would land on a solid cell; the remaining links into a
+// wall plane reflect specularly and all others stream.  Solid cells keep the
+// rest state.
 static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
 {
-    const int nx = c->nx, ny = c->ny, zd = c->nz + 2;
+    const int nx = c->nx, ny = c->ny, nz = c->nz, zd = nz + 2;
+    const bool general = c->deck.bc_mode == DNSLBM_BC_GENERAL;
     auto S = [&](int x, int y, int k) { return (int)fl[((size_t)x * ny + y) * zd + k]; };
+    std::vector<char> has_solid(nz, 0);
     for (int x = 0; x < nx; ++x)
         for (int y = 0; y < ny; ++y) {
             for (int k : {0, zd - 1}) {
@@ -348,12 +376,22 @@ static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
             }
             for (int k = 1; k < zd - 1; ++k) {
                 const int v = S(x, y, k);
+                if (v == -1 && general) {
+                    has_solid[k - 1] = 1;
+                    continue;
+                }
                 if (v != 0 && v != 1)
                     return fail(c, DNSLBM_ERR_ARG,
-                                "cell (%d,%d,%d) has flag %d; solids inside the flow are not supported by this build", x,
-                                y, k, v);
+                                general ? "cell (%d,%d,%d) has flag %d; inside the flow a cell is fluid (0, 1) or solid (-1)"
+                                        : "cell (%d,%d,%d) has flag %d; solids inside the flow need the general boundary "
+                                          "mode (DNSLBM_BC_GENERAL)",
+                                x, y, k, v);
             }
         }
+    if (c->have_state && c->odd) {
+        // the populations in flight were placed under the old flags
+        return fail(c, DNSLBM_ERR_STATE, "flags can only change between even numbers of steps");
+    }
     std::vector<uint8_t> m((size_t)2 * nx * ny);
     const int off[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
     int textured = 0;
@@ -370,14 +408,59 @@ static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
                 if (bits != 0x1f) textured = 1;
             }
     }
-    if (c->have_state && c->odd) {
-        // the populations in flight were placed under the old flags
-        return fail(c, DNSLBM_ERR_STATE, "flags can only change between even numbers of steps");
+    // planes with link masks
+    std::vector<int> band(nz, -1);
+    int nband = 0;
+    for (int z = 0; z < nz; ++z)
+        if (has_solid[z] || (z > 0 && has_solid[z - 1]) || (z + 1 < nz && has_solid[z + 1])) band[z] = nband++;
+    std::vector<unsigned> lk((size_t)nband * ny * nx, 0u);
+    for (int z = 0; z < nz; ++z) {
+        if (band[z] < 0) continue;
+        const int k = z + 1;
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                unsigned v = 0;
+                if (S(x, y, k) == -1) {
+                    v = 1u;
+                } else {
+                    for (int a = 1; a < Q; ++a) {
+                        const int xt = (x + lat_ex(a) + nx) % nx, yt = (y + lat_ey(a) + ny) % ny, kt = k + lat_ez(a);
+                        const int sld = S(xt, yt, kt), sld1 = S(x, y, kt);
+                        bool bounce;
+                        if (sld > -1) bounce = false;
+                        else if (sld == -1 && sld1 == -1) bounce = true;
+                        else if ((sld == -1 && sld1 == -2) || sld == -2) bounce = S(xt, yt, k) == -1;
+                        else bounce = true;
+                        if (bounce) v |= 1u << a;
+                    }
+                }
+                lk[((size_t)band[z] * ny + y) * nx + x] = v;
+            }
     }
+    if (nband > 0) textured = 2;
     CK(cudaSetDevice(c->deck.device));
+    const size_t lbytes = lk.size() * sizeof(unsigned);
+    if (lbytes > c->links_bytes) {
+        if (c->links) CK(cudaFree(c->links));
+        c->links = nullptr;
+        c->links_bytes = 0;
+        cudaError_t e = cudaMalloc(&c->links, lbytes);
+        if (e != cudaSuccess) return fail(c, DNSLBM_ERR_NOMEM, "cudaMalloc of %zu bytes of link masks failed", lbytes);
+        c->links_bytes = lbytes;
+    }
     CK(cudaMemcpyAsync(c->wallmask, m.data(), m.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->band_of, band.data(), band.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    if (lbytes) CK(cudaMemcpyAsync(c->links, lk.data(), lbytes, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->textured = textured;
+    c->nband = nband;
+    if (textured == 2 && c->have_state) {
+        // cells that became solid take the rest state; the sums of the
+        // current step are taken again
+        launch_io(c->deck.precision, 4, io_args(c), 0, 0, nullptr, nullptr, c->stream);
+        CK(cudaGetLastError());
+        return initial_reduce(c);
+    }
     return DNSLBM_OK;
 }
 
@@ -493,14 +576,14 @@ static int launch_steps(dnslbm_ctx *c, long n, bool timed, double *ms_even, doub
         if (timed) CK(cudaEventRecord(c->tev[2 * s], c->stream));
         if (c->use_tma) {
             if (c->deck.precision == 64)
-                launch_tma_f64(p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd, c->textured != 0, c->stream);
+                launch_tma_f64(p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd, c->textured, c->stream);
             else
                 launch_tma_lp(c->deck.precision, p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd,
-                              c->textured != 0, c->stream);
+                              c->textured, c->stream);
         } else if (c->deck.precision == 64) {
-            launch_step_f64(p, c->grid, c->block, odd, c->textured != 0, c->stream);
+            launch_step_f64(p, c->grid, c->block, odd, c->textured, c->stream);
         } else {
-            launch_step_lp(c->deck.precision, p, c->grid, c->block, odd, c->textured != 0, c->stream);
+            launch_step_lp(c->deck.precision, p, c->grid, c->block, odd, c->textured, c->stream);
         }
         CK(cudaGetLastError());
         if (timed) CK(cudaEventRecord(c->tev[2 * s + 1], c->stream));
@@ -764,5 +847,317 @@ extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t re
     if (report && report_len)
         snprintf(report, report_len, "%s: %.4f ms/step (best of %d launch shapes, %d steps each)", c->kernel_desc,
                  best_ms, ncand, steps);
+    return DNSLBM_OK;
+}
+
+// ---------------------------------------------------------------- batches
+struct dnslbm_batch {
+    std::vector<dnslbm_ctx *> ch;
+    int precision = 64, device = 0;
+    cudaStream_t stream = nullptr;
+    ChannelLaunch *d_launch = nullptr;
+    int grid = 0, threads = 0;
+    size_t smem = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // a chunk of steps starting on an even / odd parity
+    int graph_steps = 32;
+    size_t budget = 0;  // shared-memory budget per block the stages were sized for
+    int stages = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    char err[512] = {0};
+};
+
+static int bfail(dnslbm_batch *b, int code, const char *fmt, ...)
+{
+    char *dst = b ? b->err : g_create_err;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(dst, 512, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define BCK(call)                                                                                        \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) return bfail(b, DNSLBM_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" const char *dnslbm_batch_last_error(const dnslbm_batch *b) { return b ? b->err : g_create_err; }
+
+static void destroy_graphs(dnslbm_batch *b)
+{
+    for (auto &g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+extern "C" void dnslbm_batch_destroy(dnslbm_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    destroy_graphs(b);
+    for (auto &e : b->ev)
+        if (e) cudaEventDestroy(e);
+    if (b->d_launch) cudaFree(b->d_launch);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    for (auto *c : b->ch) dnslbm_destroy(c);
+    delete b;
+}
+
+// Shared-memory budgets per block for one, two and three blocks per SM
+// (228 KB per SM, 1 KB of it reserved per block, the static shared memory of
+// the kernel on top).
+constexpr size_t kBatchBudget1 = 220 * 1024, kBatchBudget2 = 108 * 1024, kBatchBudget3 = 70 * 1024;
+
+// One launch shape for all channels: per channel the most rows per stage
+// group (1, 2, 4 or 8) whose `stages` groups fit `budget` bytes; the block
+// takes the largest of these; blocks are shared among the channels in
+// proportion to their cells.  Returns 0 and selects the shape when it runs
+// on the device.
+static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consumers)
+{
+    consumers = std::max(32, std::min(352, consumers / 32 * 32));
+    size_t smem = 0;
+    std::vector<TmaArgs> t(b->ch.size());
+    for (size_t i = 0; i < b->ch.size(); ++i) {
+        dnslbm_ctx *c = b->ch[i];
+        const int row_bytes = c->pitch * (int)c->esize;
+        auto need = [&](int k) { return (size_t)stages * Q * row_bytes * k + 16 * (size_t)stages; };
+        if (need(1) > budget) return -1;
+        int k = 1;
+        while (k < 8 && 2 * k <= c->ny && need(2 * k) <= budget) k *= 2;
+        const int gpp = (c->ny + k - 1) / k;
+        t[i] = TmaArgs{gpp * c->nz, 1, stages, row_bytes, k, gpp};
+        smem = std::max(smem, need(k));
+    }
+    const int threads = consumers + 32;
+    const int prep = b->precision == 64 ? tma_batch_prepare_f64(smem) : tma_batch_prepare_lp(b->precision, smem);
+    const int occ = prep ? 0
+                         : (b->precision == 64 ? tma_batch_occupancy_f64(threads, smem)
+                                               : tma_batch_occupancy_lp(b->precision, threads, smem));
+    cudaGetLastError();  // a failed query only rules the shape out
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+    if (occ < 1 || nsm < 1) return -1;
+    double total = 0;
+    for (auto *c : b->ch) total += (double)c->nx * c->ny * c->nz;
+    const int target = occ * nsm;
+    int grid = 0;
+    for (size_t i = 0; i < b->ch.size(); ++i) {
+        dnslbm_ctx *c = b->ch[i];
+        const double share = (double)c->nx * c->ny * c->nz / total;
+        const int want = std::max(1, (int)(target * share + 0.5));
+        t[i].groups_per_block = (t[i].ngroups + want - 1) / want;
+        c->tma = t[i];
+        c->tma_grid = (t[i].ngroups + t[i].groups_per_block - 1) / t[i].groups_per_block;
+        c->tma_threads = threads;
+        c->tma_smem = smem;
+        grid += c->tma_grid;
+    }
+    b->grid = grid;
+    b->threads = threads;
+    b->smem = smem;
+    b->budget = budget;
+    b->stages = stages;
+    destroy_graphs(b);
+    return 0;
+}
+
+extern "C" int dnslbm_batch_create(const dnslbm_deck *decks, int n, dnslbm_batch **out)
+{
+    dnslbm_batch *b = nullptr;
+    if (!decks || !out || n < 1) return bfail(b, DNSLBM_ERR_ARG, "need at least one deck and an output pointer");
+    *out = nullptr;
+    for (int i = 1; i < n; ++i)
+        if (decks[i].precision != decks[0].precision || decks[i].device != decks[0].device)
+            return bfail(b, DNSLBM_ERR_ARG, "all channels of a batch share one precision and one device");
+    b = new dnslbm_batch();
+    b->precision = decks[0].precision;
+    b->device = decks[0].device;
+    for (int i = 0; i < n; ++i) {
+        dnslbm_ctx *c = nullptr;
+        int rc = dnslbm_create(&decks[i], &c);
+        if (rc) {
+            char msg[512];
+            snprintf(msg, sizeof msg, "channel %d: %s", i, g_create_err);
+            dnslbm_batch_destroy(b);
+            snprintf(g_create_err, sizeof g_create_err, "%s", msg);
+            return rc;
+        }
+        b->ch.push_back(c);
+        if (!c->use_tma) {
+            dnslbm_batch_destroy(b);
+            snprintf(g_create_err, sizeof g_create_err,
+                     "channel %d does not fit the row-pipelined kernel (rows too long for two stages)", i);
+            return DNSLBM_ERR_ARG;
+        }
+    }
+    auto bail = [&](int code) {
+        snprintf(g_create_err, sizeof g_create_err, "%s", b->err);
+        dnslbm_batch_destroy(b);
+        return code;
+    };
+    if (cudaSetDevice(b->device) != cudaSuccess) return bail(bfail(b, DNSLBM_ERR_CUDA, "cannot select device"));
+    // default launch shape: stages sized for two blocks per SM, the widest
+    // consumer set any channel would use alone
+    int consumers = 32;
+    for (auto *c : b->ch) consumers = std::max(consumers, c->tma_threads - 32);
+    if (batch_configure(b, kBatchBudget2, 2, consumers) && batch_configure(b, kBatchBudget1, 2, consumers))
+        return bail(bfail(b, DNSLBM_ERR_ARG, "batched kernel does not fit the device"));
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess ||
+        cudaMalloc(&b->d_launch, sizeof(ChannelLaunch) * n) != cudaSuccess)
+        return bail(bfail(b, DNSLBM_ERR_CUDA, "batch set-up failed: %s", cudaGetErrorString(cudaGetLastError())));
+    *out = b;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_batch_size(const dnslbm_batch *b) { return b ? (int)b->ch.size() : 0; }
+extern "C" dnslbm_ctx *dnslbm_batch_channel(dnslbm_batch *b, int i)
+{
+    return b && i >= 0 && i < (int)b->ch.size() ? b->ch[i] : nullptr;
+}
+
+static int batch_launch(dnslbm_batch *b, bool odd)
+{
+    if (b->precision == 64)
+        launch_tma_batch_f64(b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd, b->stream);
+    else
+        launch_tma_batch_lp(b->precision, b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd,
+                            b->stream);
+    BCK(cudaGetLastError());
+    return DNSLBM_OK;
+}
+
+static int batch_run(dnslbm_batch *b, long nsteps, double *ms)
+{
+    const int n = (int)b->ch.size();
+    for (int i = 0; i < n; ++i) {
+        dnslbm_ctx *c = b->ch[i];
+        if (!c->have_state) return bfail(b, DNSLBM_ERR_STATE, "channel %d has no state", i);
+        if (c->done != b->ch[0]->done || c->odd != b->ch[0]->odd)
+            return bfail(b, DNSLBM_ERR_STATE, "channel %d is at step %lld, channel 0 at %lld", i, c->done,
+                         b->ch[0]->done);
+        if (c->stream) BCK(cudaStreamSynchronize(c->stream));
+    }
+    BCK(cudaSetDevice(b->device));
+    // launch table (flags may have changed a channel's wall mode)
+    std::vector<ChannelLaunch> h(n);
+    int first = 0;
+    for (int i = 0; i < n; ++i) {
+        dnslbm_ctx *c = b->ch[i];
+        h[i].p = step_args(c);
+        h[i].t = c->tma;
+        h[i].first_block = first;
+        h[i].textured = c->textured;
+        first += c->tma_grid;
+    }
+    BCK(cudaMemcpyAsync(b->d_launch, h.data(), sizeof(ChannelLaunch) * n, cudaMemcpyHostToDevice, b->stream));
+    int odd = b->ch[0]->odd;
+    long left = nsteps;
+    if (ms) BCK(cudaEventRecord(b->ev[0], b->stream));
+    // the time loop: chunks of graph_steps launches replayed from a CUDA graph
+    while (left >= b->graph_steps) {
+        cudaGraphExec_t &g = b->graph[odd];
+        if (!g) {
+            cudaGraph_t graph;
+            BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = DNSLBM_OK;
+            for (int s = 0; s < b->graph_steps && rc == DNSLBM_OK; ++s) rc = batch_launch(b, ((odd + s) & 1) != 0);
+            cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
+            if (rc) return rc;
+            if (ee != cudaSuccess) return bfail(b, DNSLBM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ee));
+            ee = cudaGraphInstantiate(&g, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ee != cudaSuccess) return bfail(b, DNSLBM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ee));
+        }
+        BCK(cudaGraphLaunch(g, b->stream));
+        left -= b->graph_steps;
+        odd = (odd + b->graph_steps) & 1;
+    }
+    for (; left > 0; --left) {
+        int rc = batch_launch(b, odd != 0);
+        if (rc) return rc;
+        odd ^= 1;
+    }
+    if (ms) BCK(cudaEventRecord(b->ev[1], b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (ms) {
+        float f = 0.f;
+        BCK(cudaEventElapsedTime(&f, b->ev[0], b->ev[1]));
+        *ms = f;
+    }
+    for (int i = 0; i < n; ++i) {
+        dnslbm_ctx *c = b->ch[i];
+        c->done += nsteps;
+        c->odd = (c->odd + (int)(nsteps & 1)) & 1;
+    }
+    for (int i = 0; i < n; ++i) {
+        int rc = check_status(b->ch[i]);
+        if (rc) return bfail(b, rc, "channel %d: %s", i, b->ch[i]->err);
+    }
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_batch_step(dnslbm_batch *b, long nsteps)
+{
+    if (!b || nsteps < 0) return bfail(b, DNSLBM_ERR_ARG, "bad batch or step count");
+    return batch_run(b, nsteps, nullptr);
+}
+
+extern "C" int dnslbm_batch_step_timed(dnslbm_batch *b, long nsteps, double *ms)
+{
+    if (!b || nsteps < 1 || !ms) return bfail(b, DNSLBM_ERR_ARG, "bad batch, step count or output");
+    return batch_run(b, nsteps, ms);
+}
+
+extern "C" const char *dnslbm_batch_kernel(const dnslbm_batch *b)
+{
+    static thread_local char buf[256];
+    if (!b) return "";
+    snprintf(buf, sizeof buf, "step_tma_batch_kernel<fp%d>: %zu channels, %d blocks x %d threads, %d stages, %zu B smem, "
+             "CUDA graph of %d steps", b->precision, b->ch.size(), b->grid, b->threads, b->stages, b->smem,
+             b->graph_steps);
+    return buf;
+}
+
+extern "C" int dnslbm_batch_autotune(dnslbm_batch *b, int steps, char *report, size_t report_len)
+{
+    if (!b) return bfail(b, DNSLBM_ERR_ARG, "null batch");
+    for (size_t i = 0; i < b->ch.size(); ++i)
+        if (b->ch[i]->have_state)
+            return bfail(b, DNSLBM_ERR_STATE, "autotune runs before any state is loaded (it steps rest states)");
+    if (steps < 2) steps = 2;
+    if (steps >= b->graph_steps) steps = b->graph_steps - 1;  // plain launches, no graph to capture
+    BCK(cudaSetDevice(b->device));
+    size_t bb = b->budget;
+    int bs = b->stages, bc = b->threads - 32, ncand = 0;
+    double best = 1e30;
+    for (size_t budget : {kBatchBudget1, kBatchBudget2, kBatchBudget3})
+        for (int st : {2, 3, 4})
+            for (int cons : {64, 128, 192, 256, 320}) {
+                if (batch_configure(b, budget, st, cons)) continue;
+                int rc = DNSLBM_OK;
+                for (auto *c : b->ch)
+                    if ((rc = dnslbm_init_rest(c))) return bfail(b, rc, "%s", c->err);
+                double ms = 0;
+                if ((rc = batch_run(b, 2, nullptr)) || (rc = batch_run(b, steps, &ms))) return rc;
+                ++ncand;
+                if (ms < best) best = ms, bb = budget, bs = st, bc = cons;
+            }
+    // leave the channels as created: no state, counters clear
+    for (auto *c : b->ch) {
+        int rc = reset_counters(c);
+        if (rc) return bfail(b, rc, "%s", c->err);
+        c->have_state = 0;
+    }
+    if (batch_configure(b, bb, bs, bc)) return bfail(b, DNSLBM_ERR_CUDA, "cannot restore the chosen launch shape");
+    BCK(cudaDeviceSynchronize());
+    if (report && report_len)
+        snprintf(report, report_len, "%s: %.4f ms/step (best of %d launch shapes, %d steps each)",
+                 dnslbm_batch_kernel(b), best / steps, ncand, steps);
     return DNSLBM_OK;
 }

@@ -40,11 +40,20 @@ __device__ __forceinline__ double gather_one(const IoArgs &p, const Nbr &n, int 
     return Nat<T>::ld(static_cast<const T *>(p.pop[slot]) + idx, lat_opp(A));
 }
 
+template <typename T, int A>
+__device__ __forceinline__ double gather_one_links(const IoArgs &p, const Nbr &n, int wall, unsigned lk)
+{
+    int slot, idx;
+    aa_address_links<A, true>(n, wall, lk, slot, idx);
+    return Nat<T>::ld(static_cast<const T *>(p.pop[slot]) + idx, lat_opp(A));
+}
+
 // natural populations of cell (x, y, z)
 template <typename T>
 __device__ __forceinline__ void gather_natural(const IoArgs &p, int x, int y, int z, double (&f)[Q])
 {
-    if (!p.odd) {
+    const unsigned lk = p.textured == 2 ? cell_links(p.band_of, p.links, p.nx, p.ny, x, y, z) : 0u;
+    if (!p.odd || (lk & 1u)) {  // a solid cell keeps its (symmetric) rest state in place
         const int c = (z * p.ny + y) * p.pitch + x;
 #pragma unroll
         for (int a = 0; a < Q; ++a) f[a] = Nat<T>::ld(static_cast<const T *>(p.pop[a]) + c, a);
@@ -52,6 +61,20 @@ __device__ __forceinline__ void gather_natural(const IoArgs &p, int x, int y, in
     }
     const Nbr n = make_nbr(x, y, z, p.nx, p.ny, p.pitch);
     const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    if (p.textured == 2 && p.band_of[z] >= 0) {
+#pragma unroll
+        for (int a = 0; a < Q; ++a) {
+            double v;
+            switch (a) {
+#define G1(A) case A: v = gather_one_links<T, A>(p, n, wall, lk); break;
+                G1(0) G1(1) G1(2) G1(3) G1(4) G1(5) G1(6) G1(7) G1(8) G1(9)
+                G1(10) G1(11) G1(12) G1(13) G1(14) G1(15) G1(16) G1(17) G1(18)
+#undef G1
+            }
+            f[lat_opp(a)] = v;
+        }
+        return;
+    }
     unsigned bits = 0x1fu;
     if (p.textured && wall != 0) bits = p.wallmask[(size_t)(wall > 0) * p.nx * p.ny + y * p.nx + x];
 #pragma unroll
@@ -96,8 +119,22 @@ __global__ void import_kernel(const IoArgs p, int x0, int nxc, const double *aos
     const int xl = (int)(tid / ((long long)p.nz * p.ny));
     const double *i = aos + (((size_t)xl * p.ny + y) * (p.nz + 2) + (z + 1)) * Q;
     const int c = (z * p.ny + y) * p.pitch + (x0 + xl);
+    const bool solid = p.textured == 2 && (cell_links(p.band_of, p.links, p.nx, p.ny, x0 + xl, y, z) & 1u);
 #pragma unroll
-    for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, i[a], a);
+    for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, solid ? Nat<float>::wq(a) : i[a], a);
+}
+
+// solid cells inside the flow -> rest state (after the flags change)
+template <typename T>
+__global__ void solid_rest_kernel(const IoArgs p)
+{
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long long)p.nx * p.ny * p.nz) return;
+    const int x = (int)(tid % p.nx), y = (int)((tid / p.nx) % p.ny), z = (int)(tid / ((long long)p.nx * p.ny));
+    if (!(cell_links(p.band_of, p.links, p.nx, p.ny, x, y, z) & 1u)) return;
+    const int c = (z * p.ny + y) * p.pitch + x;
+#pragma unroll
+    for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, Nat<float>::wq(a), a);
 }
 
 // rest state f = w (init.c:6-19); row padding included
@@ -235,6 +272,9 @@ static void io_dispatch(int what, const IoArgs &p, int x0, int nxc, double *a, d
     } else if (what == 2) {
         const long long n = (long long)p.pitch * p.ny * p.nz;
         rest_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p);
+    } else if (what == 4) {
+        const long long n = (long long)p.nx * p.ny * p.nz;
+        solid_rest_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p);
     } else {
         const long long n = (long long)nxc * p.ny * (p.nz + 2);
         moments_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p, x0, nxc, a, b);

@@ -26,7 +26,7 @@
 #include "step_common.cuh"
 
 namespace dnslbm {
-void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, bool textured, cudaStream_t s);
+void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex, cudaStream_t s);
 void launch_reduce_f64(const StepArgs &p, dim3 grid, dim3 block, cudaStream_t s);
 }  // namespace dnslbm
 
@@ -153,6 +153,8 @@ extern "C" int dnslbm_step_f64_noalloc(double *pop, size_t pop_stride, int xdv, 
     p.rows = rows;
     p.slots = ((xdv + bx - 1) / bx) * ((ydv + rows - 1) / rows);
     p.wallmask = wallmask;
+    p.band_of = nullptr;
+    p.links = nullptr;
     p.omega = omega;
     p.ubulk = 0.0;
     p.gx = gx;
@@ -173,7 +175,8 @@ extern "C" int dnslbm_step_f64_noalloc(double *pop, size_t pop_stride, int xdv, 
     // a state in the natural layout gets the plane means of the first step,
     // exactly as after dnslbm_load_state
     if (parity == 0) launch_reduce_f64(p, grid, block, s);
-    for (long n = 0; n < nsteps; ++n) launch_step_f64(p, grid, block, ((parity + n) & 1) != 0, wallmask != nullptr, s);
+    for (long n = 0; n < nsteps; ++n)
+        launch_step_f64(p, grid, block, ((parity + n) & 1) != 0, wallmask != nullptr ? 1 : 0, s);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(msg, sizeof msg, "step launch failed: %s", cudaGetErrorString(e));

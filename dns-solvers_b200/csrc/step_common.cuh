@@ -38,6 +38,10 @@ struct StepArgs {
     double *logs;            // [log_cap][9]
     int log_cap;
     long long *status;       // [0] first NaN step + 1 (0: none)
+    // solids inside the flow (general boundary mode): planes within one
+    // plane of a solid cell carry a per-cell link mask, see cell_links
+    const int *band_of;      // [nz] index of the plane's mask block, -1: none
+    const unsigned *links;   // [nband][ny][nx]
 };
 
 // Arguments of the state readers/writers (import, export, moments, stats).
@@ -46,9 +50,26 @@ struct IoArgs {
     int nx, ny, nz;
     int pitch;  // row pitch in elements
     const uint8_t *wallmask;
-    int textured;
+    int textured;  // 0 smooth walls, 1 textured walls, 2 solids inside the flow
     int odd;  // 1: populations are post-collision in swapped slots
+    const int *band_of;
+    const unsigned *links;
 };
+
+// Link mask of a cell in a plane next to a solid inside the flow
+// (boundary mode DNSLBM_BC_GENERAL): bit 0 set for a solid cell (never
+// collided, holds the rest state), bit A (1..18) set when the link from the
+// cell in direction A bounces back -- into a solid cell, into a no-slip wall
+// cell whose own wall cell is no-slip too, or a specular reflection whose
+// target cell is solid.  A clear bit of a link into a wall plane means
+// specular reflection; every other clear bit is plain streaming.  Cells of
+// planes without a mask block have no solid neighbour (0).
+__device__ __forceinline__ unsigned cell_links(const int *band_of, const unsigned *links, int nx, int ny, int x,
+                                               int y, int z)
+{
+    const int b = band_of[z];
+    return b < 0 ? 0u : links[((size_t)b * ny + y) * nx + x];
+}
 
 // ---------------------------------------------------------------- addresses
 // Neighbourhood of a cell: wrapped x and the 9 row offsets (dy, dz).
@@ -106,6 +127,28 @@ __device__ __forceinline__ void aa_address(const Nbr &n, int wall, unsigned bits
     }
     slot = A;
     idx = n.row[ey + 1][ez + 1] + nbr_x(n, ex);
+}
+
+// The same with a per-cell link mask (boundary mode DNSLBM_BC_GENERAL, a
+// cell that is not solid): bounce-back to slot opp(A) of the cell, specular
+// reflection for the other links into a wall plane, else plain streaming.
+template <int A, bool ODD>
+__device__ __forceinline__ void aa_address_links(const Nbr &n, int wall, unsigned links, int &slot, int &idx)
+{
+    constexpr int ex = lat_ex(A), ey = lat_ey(A), ez = lat_ez(A);
+    if (!ODD || A == 0) {
+        slot = A;
+        idx = n.c0;
+    } else if ((links >> A) & 1u) {
+        slot = lat_opp(A);
+        idx = n.c0;
+    } else if (ez != 0 && wall == ez) {
+        slot = lat_mir(A);
+        idx = n.row[ey + 1][1] + nbr_x(n, ex);
+    } else {
+        slot = A;
+        idx = n.row[ey + 1][ez + 1] + nbr_x(n, ex);
+    }
 }
 
 // ---------------------------------------------------------------- reduction

@@ -9,6 +9,7 @@
 // signed zero to a non-zero partial sum leaves it unchanged.
 #include "collide_f64.cuh"
 #include "step_common.cuh"
+#include "step_links.cuh"
 
 namespace dnslbm {
 
@@ -20,7 +21,7 @@ __device__ __forceinline__ double *f64_ptr(const StepArgs &p, const Nbr &n, int 
     return static_cast<double *>(p.pop[slot]) + idx;
 }
 
-template <bool ODD, bool CONSTQ, bool TEXTURED>
+template <bool ODD, bool CONSTQ, int TEX>
 __global__ void __launch_bounds__(128, 4) step_f64_kernel(const StepArgs p)
 {
     const long long step = *p.step_ctr;
@@ -41,7 +42,15 @@ __global__ void __launch_bounds__(128, 4) step_f64_kernel(const StepArgs p)
         for (int y = y0; y < y1; ++y) {
             const Nbr n = make_nbr(x, y, z, p.nx, p.ny, p.pitch);
             unsigned bits = 0x1fu;
-            if (TEXTURED && wall != 0) bits = p.wallmask[(size_t)(wall > 0) * p.nx * p.ny + y * p.nx + x];
+            if (TEX != 0 && wall != 0) bits = p.wallmask[(size_t)(wall > 0) * p.nx * p.ny + y * p.nx + x];
+            if (TEX == 2 && p.band_of[z] >= 0) {  // plane next to a solid: per-cell links
+                float racc[NP] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                links_cell<double, ODD, CONSTQ>(p, n, wall, cell_links(p.band_of, p.links, p.nx, p.ny, x, y, z), nullptr, 0,
+                                          G, c0, c1, c2, acc, racc);
+#pragma unroll
+                for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i];
+                continue;
+            }
             double f[Q];
 #pragma unroll
             for (int a = 0; a < Q; ++a) {
@@ -127,17 +136,17 @@ __global__ void __launch_bounds__(128) reduce_f64_kernel(const StepArgs p)
     block_epilogue(p, acc, step, 0.0, 1);
 }
 
-void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, bool textured, cudaStream_t s)
+void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex, cudaStream_t s)
 {
     const bool q = p.const_q != 0;
 #define L(O, C, T) step_f64_kernel<O, C, T><<<grid, block, 0, s>>>(p)
+#define LX(O, C) do { if (tex == 2) L(O, C, 2); else if (tex) L(O, C, 1); else L(O, C, 0); } while (0)
     if (odd) {
-        if (q) { if (textured) L(true, true, true); else L(true, true, false); }
-        else   { if (textured) L(true, false, true); else L(true, false, false); }
+        if (q) LX(true, true); else LX(true, false);
     } else {
-        if (q) { if (textured) L(false, true, true); else L(false, true, false); }
-        else   { if (textured) L(false, false, true); else L(false, false, false); }
+        if (q) LX(false, true); else LX(false, false);
     }
+#undef LX
 #undef L
 }
 

@@ -23,7 +23,11 @@
 // back to the cell's own slot opp(A), again a whole own row (bulk).  With a
 // textured wall the five links into the wall go to rows that several cell
 // rows share (bounce-back or specular per cell), so those five are moved by
-// per-thread loads/stores and never by a bulk copy.
+// per-thread loads/stores and never by a bulk copy.  Planes next to solids
+// inside the flow (TEX 2) move all 19 per thread in an odd step
+// (step_links.cuh); their even step is bulk like any other.
+//
+// TEX: 0 smooth walls, 1 textured walls, 2 solids inside the flow.
 //
 // Every wait on an mbarrier is bounded; a wait that runs out records
 // status[1] and a shared abort flag, after which no thread of the block waits
@@ -37,6 +41,7 @@
 #include "collide_f64.cuh"
 #include "collide_lp.cuh"
 #include "step_common.cuh"
+#include "step_links.cuh"
 
 namespace dnslbm {
 
@@ -118,7 +123,7 @@ struct GroupRows {
     bool bulk;
 };
 
-template <bool ODD, bool TEXTURED>
+template <bool ODD, int TEX>
 __device__ __forceinline__ GroupRows group_rows(const StepArgs &p, int A, int y0, int z, int wall)
 {
     GroupRows g;
@@ -126,8 +131,11 @@ __device__ __forceinline__ GroupRows group_rows(const StepArgs &p, int A, int y0
     g.bulk = true;
     if (!ODD) {
         g.slot = A; g.zz = z; g.y_first = y0;
+    } else if (TEX == 2 && p.band_of[z] >= 0) {
+        g.bulk = false;  // plane next to a solid: every link per thread
+        g.slot = A; g.zz = z; g.y_first = y0;
     } else if (ez != 0 && ez == wall) {
-        g.bulk = !TEXTURED;
+        g.bulk = TEX == 0;
         g.slot = lat_opp(A); g.zz = z; g.y_first = y0;  // bounce-back to the cell's own rows
     } else {
         g.slot = A; g.zz = z + ez; g.y_first = y0 + lat_ey(A);
@@ -161,22 +169,6 @@ __device__ __forceinline__ void copy_group(const StepArgs &p, const TmaArgs &t, 
 }
 
 // ------------------------------------------------------------------ cells
-template <typename T>
-using RegT = typename std::conditional<std::is_same<T, double>::value, double, float>::type;
-
-template <typename T>
-__device__ __forceinline__ RegT<T> ld_raw(const T *q)
-{
-    if constexpr (std::is_same<T, double>::value) return *q;
-    else return LpStore<T>::ld(q);
-}
-template <typename T>
-__device__ __forceinline__ void st_raw(T *q, RegT<T> v)
-{
-    if constexpr (std::is_same<T, double>::value) *q = v;
-    else LpStore<T>::st(q, v);
-}
-
 // One cell row from the stage buffer: direction A's element x at
 // sb[A * dstride + x].
 // WALL: 0 interior plane, -1 bottom plane, +1 top plane.
@@ -300,10 +292,31 @@ __device__ __forceinline__ void tma_row(const StepArgs &p, T *sb, int dstride, i
     }
 }
 
+// One cell row of a plane next to a solid (TEX 2): per-cell link masks.
+template <typename T, bool ODD, bool CONSTQ>
+__device__ __forceinline__ void links_row(const StepArgs &p, T *sb, int dstride, int y, int z, double G,
+                                          const double *shift, double (&acc)[NP], int nc)
+{
+    const int nx = p.nx, wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const unsigned *lrow = p.links + ((size_t)p.band_of[z] * p.ny + y) * nx;
+    float racc[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) racc[i] = 0.f;
+    for (int x = threadIdx.x; x < nx; x += nc) {
+        const Nbr n = make_nbr(x, y, z, nx, p.ny, p.pitch);
+        links_cell<T, ODD, CONSTQ>(p, n, wall, lrow[x], ODD ? nullptr : sb + x, dstride, G, shift[0], shift[1],
+                                   shift[2], acc, racc);
+    }
+    if constexpr (!std::is_same<T, double>::value) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i];
+    }
+}
+
 // ------------------------------------------------------------------ kernel
 // Producer warp: lane A < 19 moves direction A's rows of every row group of
 // the block; lane 0 also arms the stage's full barrier with the byte count.
-template <typename T, bool ODD, bool TEXTURED>
+template <typename T, bool ODD, int TEX>
 __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t, int g0, int n, int lane,
                                              unsigned char *smem, uint64_t *full, uint64_t *empty, volatile int *abort)
 {
@@ -321,7 +334,7 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             const int k = min(t.k, p.ny - y0);
             const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
             if (lane < Q && !*abort) {
-                const GroupRows g = group_rows<ODD, TEXTURED>(p, lane, y0, z, wall);
+                const GroupRows g = group_rows<ODD, TEX>(p, lane, y0, z, wall);
                 if (g.bulk) copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, false, nullptr);
                 bulk_commit();
             }
@@ -331,7 +344,7 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             const int k = min(t.k, p.ny - y0);
             const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
             GroupRows g{};
-            if (lane < Q) g = group_rows<ODD, TEXTURED>(p, lane, y0, z, wall);
+            if (lane < Q) g = group_rows<ODD, TEX>(p, lane, y0, z, wall);
             const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && g.bulk);
             if (lane < Q) bulk_wait_read_all();  // this lane's store of the stage has read it
             __syncwarp();
@@ -346,13 +359,14 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
 
 constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer warp
 
-template <typename T, bool ODD, bool CONSTQ, bool TEXTURED>
-__global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepArgs p, const TmaArgs t)
+// The step of one channel by one block: `blk` numbers the block among the
+// channel's blocks, `tma_smem` is the block's dynamic shared memory.
+template <typename T, bool ODD, bool CONSTQ, int TEX>
+__device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &t, int blk, unsigned char *tma_smem)
 {
-    extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ int s_abort;
     const int G_ = t.groups_per_block, S = t.stages;
-    const int g0 = blockIdx.x * G_;
+    const int g0 = blk * G_;
     const int n = min(g0 + G_, t.ngroups) - g0;
     if (n <= 0) return;  // block-uniform; empty blocks contribute to no plane
     const int nc = blockDim.x - 32;  // consumer threads; the last warp produces
@@ -369,7 +383,7 @@ __global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepA
     }
     __syncthreads();
     if (threadIdx.x >= nc) {
-        tma_producer<T, ODD, TEXTURED>(p, t, g0, n, threadIdx.x - nc, tma_smem, full, empty, &s_abort);
+        tma_producer<T, ODD, TEX>(p, t, g0, n, threadIdx.x - nc, tma_smem, full, empty, &s_abort);
         return;
     }
 
@@ -390,11 +404,14 @@ __global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepA
         }
         T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
         const double *sh = shift_now + z * 3;
+        constexpr bool TXT = TEX != 0;
+        const bool links = TEX == 2 && p.band_of[z] >= 0;
         for (int j = 0; j < k; ++j) {
             T *sbj = sb + (size_t)j * p.pitch;
-            if (z == 0) tma_row<T, ODD, CONSTQ, TEXTURED, -1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
-            else if (z == p.nz - 1) tma_row<T, ODD, CONSTQ, TEXTURED, 1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
-            else tma_row<T, ODD, CONSTQ, TEXTURED, 0>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+            if (links) links_row<T, ODD, CONSTQ>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+            else if (z == 0) tma_row<T, ODD, CONSTQ, TXT, -1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+            else if (z == p.nz - 1) tma_row<T, ODD, CONSTQ, TXT, 1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+            else tma_row<T, ODD, CONSTQ, TXT, 0>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
         }
         fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         __syncwarp();
@@ -402,10 +419,59 @@ __global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepA
         if (i + 1 == n || (gi + 1) % t.gpp == 0) {  // this block's last group of plane z
             const int bfirst = (z * t.gpp) / G_;
             const int blast = min(((z + 1) * t.gpp - 1) / G_, (t.ngroups - 1) / G_);
-            plane_contribute(p, acc, z, blockIdx.x - bfirst, blast - bfirst + 1, step, G, 0, nc);
+            plane_contribute(p, acc, z, blk - bfirst, blast - bfirst + 1, step, G, 0, nc);
 #pragma unroll
             for (int q = 0; q < NP; ++q) acc[q] = 0.0;
         }
+    }
+}
+
+template <typename T, bool ODD, bool CONSTQ, int TEX>
+__global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepArgs p, const TmaArgs t)
+{
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    tma_step_body<T, ODD, CONSTQ, TEX>(p, t, blockIdx.x, tma_smem);
+}
+
+// Many independent channels in one launch: block b belongs to the channel c
+// with first[c] <= b < first[c+1]; the channel's arguments are copied to
+// shared memory and the block runs that channel's step.
+struct ChannelLaunch {
+    StepArgs p;
+    TmaArgs t;
+    int first_block;
+    int textured;  // TEX of the channel
+};
+
+template <typename T, bool ODD>
+__global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_batch_kernel(const ChannelLaunch *__restrict__ chans,
+                                                                           int nchan)
+{
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    __shared__ ChannelLaunch L;
+    __shared__ int s_c;
+    if (threadIdx.x == 0) {
+        int c = 0;
+        while (c + 1 < nchan && chans[c + 1].first_block <= (int)blockIdx.x) ++c;
+        s_c = c;
+    }
+    __syncthreads();
+    {
+        const int *src = reinterpret_cast<const int *>(chans + s_c);
+        int *dst = reinterpret_cast<int *>(&L);
+        for (int i = threadIdx.x; i < (int)(sizeof(ChannelLaunch) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const int blk = blockIdx.x - L.first_block;
+    const bool q = L.p.const_q != 0;
+    if (q) {
+        if (L.textured == 2) tma_step_body<T, ODD, true, 2>(L.p, L.t, blk, tma_smem);
+        else if (L.textured) tma_step_body<T, ODD, true, 1>(L.p, L.t, blk, tma_smem);
+        else tma_step_body<T, ODD, true, 0>(L.p, L.t, blk, tma_smem);
+    } else {
+        if (L.textured == 2) tma_step_body<T, ODD, false, 2>(L.p, L.t, blk, tma_smem);
+        else if (L.textured) tma_step_body<T, ODD, false, 1>(L.p, L.t, blk, tma_smem);
+        else tma_step_body<T, ODD, false, 0>(L.p, L.t, blk, tma_smem);
     }
 }
 
@@ -413,10 +479,12 @@ template <typename T>
 int tma_set_smem_attr(size_t bytes)
 {
     const void *ks[] = {
-        (const void *)step_tma_kernel<T, false, false, false>, (const void *)step_tma_kernel<T, false, false, true>,
-        (const void *)step_tma_kernel<T, false, true, false>,  (const void *)step_tma_kernel<T, false, true, true>,
-        (const void *)step_tma_kernel<T, true, false, false>,  (const void *)step_tma_kernel<T, true, false, true>,
-        (const void *)step_tma_kernel<T, true, true, false>,   (const void *)step_tma_kernel<T, true, true, true>};
+        (const void *)step_tma_kernel<T, false, false, 0>, (const void *)step_tma_kernel<T, false, false, 1>,
+        (const void *)step_tma_kernel<T, false, false, 2>, (const void *)step_tma_kernel<T, false, true, 0>,
+        (const void *)step_tma_kernel<T, false, true, 1>,  (const void *)step_tma_kernel<T, false, true, 2>,
+        (const void *)step_tma_kernel<T, true, false, 0>,  (const void *)step_tma_kernel<T, true, false, 1>,
+        (const void *)step_tma_kernel<T, true, false, 2>,  (const void *)step_tma_kernel<T, true, true, 0>,
+        (const void *)step_tma_kernel<T, true, true, 1>,   (const void *)step_tma_kernel<T, true, true, 2>};
     for (const void *k : ks)
         if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return -1;
     return 0;
@@ -426,26 +494,53 @@ template <typename T>
 int tma_occupancy(int threads, size_t smem)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, false>, threads, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0>, threads, smem) !=
         cudaSuccess)
         return 0;
     return n;
 }
 
 template <typename T>
-void launch_tma(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, bool textured,
+void launch_tma(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
                 cudaStream_t s)
 {
     const bool q = p.const_q != 0;
 #define L(O, C, X) step_tma_kernel<T, O, C, X><<<grid, threads, smem, s>>>(p, t)
+#define LX(O, C) do { if (tex == 2) L(O, C, 2); else if (tex) L(O, C, 1); else L(O, C, 0); } while (0)
     if (odd) {
-        if (q) { if (textured) L(true, true, true); else L(true, true, false); }
-        else   { if (textured) L(true, false, true); else L(true, false, false); }
+        if (q) LX(true, true); else LX(true, false);
     } else {
-        if (q) { if (textured) L(false, true, true); else L(false, true, false); }
-        else   { if (textured) L(false, false, true); else L(false, false, false); }
+        if (q) LX(false, true); else LX(false, false);
     }
+#undef LX
 #undef L
+}
+
+template <typename T>
+int tma_batch_set_smem_attr(size_t bytes)
+{
+    const void *ks[] = {(const void *)step_tma_batch_kernel<T, false>, (const void *)step_tma_batch_kernel<T, true>};
+    for (const void *k : ks)
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return -1;
+    return 0;
+}
+
+template <typename T>
+int tma_batch_occupancy(int threads, size_t smem)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_batch_kernel<T, true>, threads, smem) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+
+template <typename T>
+void launch_tma_batch(const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem, bool odd,
+                      cudaStream_t s)
+{
+    if (odd) step_tma_batch_kernel<T, true><<<grid, threads, smem, s>>>(chans, nchan);
+    else step_tma_batch_kernel<T, false><<<grid, threads, smem, s>>>(chans, nchan);
 }
 
 }  // namespace dnslbm

@@ -6,10 +6,18 @@ namespace dnslbm {
 
 int tma_prepare_f64(size_t smem) { return tma_set_smem_attr<double>(smem); }
 int tma_occupancy_f64(int threads, size_t smem) { return tma_occupancy<double>(threads, smem); }
-void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, bool textured,
+void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
                     cudaStream_t s)
 {
-    launch_tma<double>(p, t, grid, threads, smem, odd, textured, s);
+    launch_tma<double>(p, t, grid, threads, smem, odd, tex, s);
+}
+
+int tma_batch_prepare_f64(size_t smem) { return tma_batch_set_smem_attr<double>(smem); }
+int tma_batch_occupancy_f64(int threads, size_t smem) { return tma_batch_occupancy<double>(threads, smem); }
+void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem, bool odd,
+                          cudaStream_t s)
+{
+    launch_tma_batch<double>(chans, nchan, grid, threads, smem, odd, s);
 }
 
 }  // namespace dnslbm

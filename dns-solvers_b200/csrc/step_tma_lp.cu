@@ -12,10 +12,25 @@ int tma_occupancy_lp(int precision, int threads, size_t smem)
     return precision == 32 ? tma_occupancy<float>(threads, smem) : tma_occupancy<__half>(threads, smem);
 }
 void launch_tma_lp(int precision, const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd,
-                   bool textured, cudaStream_t s)
+                   int tex, cudaStream_t s)
 {
-    if (precision == 32) launch_tma<float>(p, t, grid, threads, smem, odd, textured, s);
-    else launch_tma<__half>(p, t, grid, threads, smem, odd, textured, s);
+    if (precision == 32) launch_tma<float>(p, t, grid, threads, smem, odd, tex, s);
+    else launch_tma<__half>(p, t, grid, threads, smem, odd, tex, s);
+}
+
+int tma_batch_prepare_lp(int precision, size_t smem)
+{
+    return precision == 32 ? tma_batch_set_smem_attr<float>(smem) : tma_batch_set_smem_attr<__half>(smem);
+}
+int tma_batch_occupancy_lp(int precision, int threads, size_t smem)
+{
+    return precision == 32 ? tma_batch_occupancy<float>(threads, smem) : tma_batch_occupancy<__half>(threads, smem);
+}
+void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem,
+                         bool odd, cudaStream_t s)
+{
+    if (precision == 32) launch_tma_batch<float>(chans, nchan, grid, threads, smem, odd, s);
+    else launch_tma_batch<__half>(chans, nchan, grid, threads, smem, odd, s);
 }
 
 }  // namespace dnslbm

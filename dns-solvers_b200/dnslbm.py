@@ -77,6 +77,19 @@ def lib():
     L.dnslbm_bytes_per_cell.argtypes = [vp]
     L.dnslbm_bytes_per_cell.restype = ctypes.c_double
     L.dnslbm_sync.argtypes = [vp]
+    L.dnslbm_batch_create.argtypes = [ctypes.POINTER(Deck), ctypes.c_int, ctypes.POINTER(vp)]
+    L.dnslbm_batch_destroy.argtypes = [vp]
+    L.dnslbm_batch_destroy.restype = None
+    L.dnslbm_batch_last_error.argtypes = [vp]
+    L.dnslbm_batch_last_error.restype = ctypes.c_char_p
+    L.dnslbm_batch_size.argtypes = [vp]
+    L.dnslbm_batch_channel.argtypes = [vp, ctypes.c_int]
+    L.dnslbm_batch_channel.restype = vp
+    L.dnslbm_batch_step.argtypes = [vp, ctypes.c_long]
+    L.dnslbm_batch_step_timed.argtypes = [vp, ctypes.c_long, dp]
+    L.dnslbm_batch_kernel.argtypes = [vp]
+    L.dnslbm_batch_kernel.restype = ctypes.c_char_p
+    L.dnslbm_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     L.dnslbm_host_alloc.argtypes = [ctypes.c_size_t]
     L.dnslbm_host_alloc.restype = vp
     L.dnslbm_host_free.argtypes = [vp]
@@ -208,6 +221,76 @@ class Channel:
 
     def sync(self):
         self._ck(self.L.dnslbm_sync(self.h))
+
+
+class _Borrowed(Channel):
+    """A channel owned by a Batch (destroyed with the batch, not alone)."""
+
+    def __init__(self, L, h, shape, deck):
+        self.L, self.h, self.shape, self.deck = L, h, shape, deck
+
+    def close(self):
+        self.h = None
+
+    __del__ = close
+
+
+def deck(xdv, ydv, zdv, omega, ubulk=0.0, gx=0.0, force_mode=CONST_G, precision=F64, bc_mode=BC_REFERENCE,
+         log_capacity=0, device=0):
+    return Deck(xdv, ydv, zdv, omega, ubulk, gx, force_mode, precision, bc_mode, log_capacity, device)
+
+
+class Batch:
+    """Many independent channels stepped by one launch per step, the time
+    loop replayed from a CUDA graph (dnslbm_batch_*)."""
+
+    def __init__(self, decks):
+        self.L = lib()
+        arr = (Deck * len(decks))(*decks)
+        h = ctypes.c_void_p()
+        rc = self.L.dnslbm_batch_create(arr, len(decks), ctypes.byref(h))
+        if rc:
+            raise DnsLbmError(rc, self.L.dnslbm_batch_last_error(None).decode())
+        self.h = h
+        self.channels = [_Borrowed(self.L, ctypes.c_void_p(self.L.dnslbm_batch_channel(h, i)),
+                                   (d.xdv, d.ydv, d.zdv), d) for i, d in enumerate(decks)]
+
+    def _ck(self, rc):
+        if rc:
+            raise DnsLbmError(rc, self.L.dnslbm_batch_last_error(self.h).decode())
+
+    def step(self, n=1):
+        self._ck(self.L.dnslbm_batch_step(self.h, n))
+
+    def step_timed(self, n):
+        ms = ctypes.c_double()
+        self._ck(self.L.dnslbm_batch_step_timed(self.h, n, ctypes.byref(ms)))
+        return ms.value
+
+    @property
+    def kernel(self):
+        return self.L.dnslbm_batch_kernel(self.h).decode()
+
+    def autotune(self, steps=8):
+        """Pick the fastest launch shape on rest states; before any load."""
+        buf = ctypes.create_string_buffer(512)
+        self._ck(self.L.dnslbm_batch_autotune(self.h, steps, buf, 512))
+        return buf.value.decode()
+
+    def close(self):
+        if getattr(self, "h", None):
+            for c in self.channels:
+                c.close()
+            self.L.dnslbm_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class PinnedArray:

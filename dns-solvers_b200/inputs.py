@@ -126,6 +126,29 @@ def flags_posts(nx, ny, nz, gx=2, wx=2, gy=2, wy=2):
     return f
 
 
+def riblet_profile(ny, height, spacing):
+    """Solid cells per spanwise index of triangular streamwise riblets: a cell
+    of wall distance k - 1/2 (k = 1 the first fluid plane; the halfway wall
+    sits at 0) is solid when it lies below the triangle of the given height
+    whose base spans one spacing, h(y) = height (1 - |2 y_c / spacing - 1|)
+    with y_c = (y mod spacing) + 1/2."""
+    yc = (np.arange(ny) % spacing) + 0.5
+    h = height * (1.0 - np.abs(2.0 * yc / spacing - 1.0))
+    return (np.ceil(h + 0.5) - 1).astype(int)  # number of planes k >= 1 with k - 1/2 < h
+
+
+def flags_riblets(nx, ny, nz, height, spacing):
+    """Triangular riblets aligned with the flow cut into both no-slip walls
+    (solid cells -1 inside the flow; boundary mode DNSLBM_BC_GENERAL)."""
+    f = flags_smooth(nx, ny, nz)
+    nk = riblet_profile(ny, height, spacing)
+    for y in range(ny):
+        if nk[y] > 0:
+            f[:, y, 1:1 + nk[y]] = -1
+            f[:, y, nz + 1 - nk[y]:nz + 1] = -1
+    return f
+
+
 def grooves_pitch(pitch, gas_fraction):
     """(gap, width) of a groove texture of the given pitch and gas fraction."""
     gap = int(round(pitch * gas_fraction))
@@ -151,21 +174,60 @@ class Workload:
         return self.nx * self.ny * self.nz
 
 
-def channel_180(h=100, texture="smooth", **tex):
-    """Re_tau ~ 180 channel of half-height h: (2 pi h) x (2h + 2) x (pi h),
-    u_tau = 0.005, nu = u_tau h / 180, tau = 0.5 + 3 nu, g = u_tau^2 / h."""
+def channel(h=100, re_tau=180.0, texture="smooth", name=None, **tex):
+    """Channel of half-height h at friction Reynolds number re_tau:
+    (2 pi h) x (2h + 2) x (pi h), u_tau = 0.005, nu = u_tau h / re_tau,
+    tau = 0.5 + 3 nu, g = u_tau^2 / h."""
     utau = 0.005
-    nu = utau * h / 180.0
+    nu = utau * h / re_tau
     tau = 0.5 + 3 * nu
     nx, ny, nz = round(2 * math.pi * h), round(math.pi * h), 2 * h
-    return Workload(f"channel_re180_h{h}", nx, ny, nz, 1.0 / tau, utau ** 2 / h, 15.7 * utau, 20, texture, tex)
+    ub = 15.7 * utau * (re_tau / 180.0) ** (1 / 7)  # bulk velocity, 1/7 power law
+    return Workload(name or f"channel_re{re_tau:g}_h{h}", nx, ny, nz, 1.0 / tau, utau ** 2 / h, ub, 20, texture, tex)
+
+
+def channel_180(h=100, texture="smooth", **tex):
+    """Re_tau ~ 180 channel of half-height h."""
+    return channel(h, 180.0, texture, name=f"channel_re180_h{h}", **tex)
+
+
+BATCH_HEIGHTS = (20, 32, 48, 64)
+
+
+def batch_channels(n=24, seed=0):
+    """n independent channels with half-heights cycling through 20, 32, 48,
+    64, and per channel (numpy PCG64, seed + index): Re_tau uniform in
+    [120, 180] and a wall texture drawn from smooth walls, longitudinal
+    grooves (pitch 8-32, gas fraction 0.5-0.9), transverse grooves (pitch 16,
+    gas fraction 0.5) and triangular riblets (height 4-8, spacing twice the
+    height)."""
+    out = []
+    for i in range(n):
+        rng = np.random.Generator(np.random.PCG64(seed + i))
+        h = BATCH_HEIGHTS[i % len(BATCH_HEIGHTS)]
+        re = float(rng.uniform(120.0, 180.0))
+        kind = ("smooth", "longitudinal", "transverse", "riblets")[int(rng.integers(4))]
+        if kind == "longitudinal":
+            gap, width = grooves_pitch(int(rng.integers(8, 33)), float(rng.uniform(0.5, 0.9)))
+            tex = {"gap": max(gap, 1), "width": max(width, 1)}
+        elif kind == "transverse":
+            tex = dict(zip(("gap", "width"), grooves_pitch(16, 0.5)))
+        elif kind == "riblets":
+            height = int(rng.integers(4, 9))
+            tex = {"height": height, "spacing": 2 * height}
+        else:
+            tex = {}
+        out.append(channel(h, re, kind, name=f"batch{i:02d}_h{h}_re{re:.0f}_{kind}", **tex))
+    return out
 
 
 def workload(name):
     """The reference-shaped workloads: 'laminar64' (64 x 66 x 32, tau 0.52,
     g 1e-6, 1000 steps), 'channel180' (628 x 202 x 314, Re_tau 180),
     'grooves180' (the same with pitch-32, gas-fraction-0.5 longitudinal
-    grooves on both walls)."""
+    grooves on both walls), 'riblets180' (the same grid with triangular
+    riblets of height 8 and spacing 16 cut into both walls) and 'riblets395'
+    (Re_tau 395, h = 200: 1256 x 408 x 628 with the same riblets)."""
     if name == "laminar64":
         return Workload("laminar64", 64, 32, 64, 1.0 / 0.52, 1e-6, 0.0, 1000)
     if name == "channel180":
@@ -175,6 +237,12 @@ def workload(name):
     if name == "grooves180":
         g, w = grooves_pitch(32, 0.5)
         return channel_180(100, "longitudinal", gap=g, width=w)
+    if name == "riblets180":  # the Re_tau 180 grid with riblets of height 8, spacing 16
+        return channel(100, 180.0, "riblets", name="riblets_re180_h100", height=8, spacing=16)
+    if name == "riblets395":  # 1256 x 408 x 628 incl. walls, riblets of height 8, spacing 16
+        w = channel(200, 395.0, "riblets", name="riblets_re395_h200", height=8, spacing=16)
+        w.nx, w.nz = 1256, 406  # the riblets take the first planes at each wall
+        return w
     raise KeyError(name)
 
 
@@ -187,7 +255,23 @@ def make_flags(wl: Workload):
         return flags_transverse(wl.nx, wl.ny, wl.nz, wl.tex["gap"], wl.tex["width"])
     if wl.texture == "posts":
         return flags_posts(wl.nx, wl.ny, wl.nz, **wl.tex)
+    if wl.texture == "riblets":
+        return flags_riblets(wl.nx, wl.ny, wl.nz, wl.tex["height"], wl.tex["spacing"])
     raise KeyError(wl.texture)
+
+
+def needs_general(wl: Workload):
+    """True when the walls put solid cells inside the flow."""
+    return wl.texture == "riblets"
+
+
+def rest_solids(state, flags):
+    """The state with every solid cell inside the flow at rest (f = w); the
+    wall planes are left as they are."""
+    s = state.copy()
+    inner = s[:, :, 1:-1]
+    inner[flags[:, :, 1:-1] == -1] = W
+    return s
 
 
 def make_state(wl: Workload, seed=0):

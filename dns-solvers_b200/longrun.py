@@ -1,0 +1,150 @@
+#!/usr/bin/env python3
+"""Long-run precision comparison: the same seeded channel advanced in FP64,
+FP32 and FP16 storage, with time-averaged statistics compared against the
+FP64 run (the FP64 kernel is bit-identical to the CPU oracle).
+
+    python dns-solvers_b200/longrun.py --workload channel180 --spinup 20000 \
+        --steps 50000 --sample 100 --out longrun.json
+
+Turbulence is chaotic: two runs that differ in the last bit decorrelate
+within a few thousand steps, and their window averages then differ by the
+sampling error of the window.  The control run "64p" (FP64 from the same
+field with every population perturbed by a seeded relative 1e-12) measures
+that floor; an FP32/FP16 error at the level of the control's is sampling
+noise, not a precision bias.
+
+Averaged over the window (after --spinup steps), per run:
+  * the per-step wall shear stress (wshearstr.c:271) -> u_tau = sqrt(tau_w/rho),
+    Re_tau = u_tau h / nu (h = zdv/2, nu = (2/omega - 1)/6);
+  * the flow rate (encalc.c:132) -> bulk velocity and skin friction
+    C_f = 2 tau_w / (rho U_b^2);
+  * the plane statistics (statistics.c) sampled every --sample steps: mean
+    u(z) and rms u'(z), v'(z), w'(z) profiles;
+  * for textured walls, the mean streamwise velocity in the first fluid plane
+    over slip and over no-slip wall cells at the end of the window.
+Errors against FP64: max |profile - profile_64| / max |profile_64| and the
+relative differences of Re_tau, C_f, U_b.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import dnslbm  # noqa: E402
+import inputs  # noqa: E402
+
+
+def run_one(wl, s0, flags, prec, spinup, steps, sample, device=0):
+    bc = dnslbm.BC_GENERAL if inputs.needs_general(wl) else dnslbm.BC_REFERENCE
+    ch = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, gx=wl.gx, force_mode=dnslbm.CONST_G, precision=prec,
+                        bc_mode=bc, device=device)
+    ch.autotune()
+    ch.set_flags(flags)
+    ch.load_state(s0)
+    t0 = time.perf_counter()
+    left = spinup
+    while left > 0:
+        n = min(4000, left)
+        ch.step(n)
+        left -= n
+    stress, flow, rho, stats = [], [], [], []
+    done = 0
+    while done < steps:
+        n = min(sample, steps - done)
+        first = ch.steps_done
+        ch.step(n)
+        lg = ch.logs(first, n)
+        stress.append(lg[:, dnslbm.LOG_NAMES.index("stress")])
+        flow.append(lg[:, dnslbm.LOG_NAMES.index("flowrate")])
+        rho.append(lg[:, dnslbm.LOG_NAMES.index("rho")])
+        done += n
+        stats.append(ch.statistics())
+    secs = time.perf_counter() - t0
+    vel, _ = ch.moments()
+    ch.close()
+    stress, flow, rho = np.concatenate(stress), np.concatenate(flow), np.concatenate(rho)
+    st = np.mean(stats, axis=0)
+    nu = (2.0 / wl.omega - 1.0) / 6.0
+    h = wl.nz / 2.0
+    tau_w = float(np.mean(stress))
+    rho_m = float(np.mean(rho))
+    utau = math.sqrt(abs(tau_w) / rho_m)
+    ub = float(np.mean(flow)) / (wl.ny * wl.nz)
+    out = {"precision": prec, "seconds": round(secs, 2), "tau_w": tau_w, "u_tau": utau, "re_tau": utau * h / nu,
+           "u_bulk": ub, "cf": 2 * tau_w / (rho_m * ub * ub), "mean_u": st[0, 1:-1], "u_rms": st[3, 1:-1],
+           "v_rms": st[4, 1:-1], "w_rms": st[5, 1:-1]}
+    slip = flags[:, :, 0] == -2
+    if slip.any():
+        u1 = vel[:, :, 1, 0]
+        out["slip_u_first_plane"] = float(u1[slip].mean())
+        out["noslip_u_first_plane"] = float(u1[~slip].mean())
+    return out
+
+
+def compare(ref, o):
+    def prof(k):
+        return float(np.max(np.abs(o[k] - ref[k])) / max(np.max(np.abs(ref[k])), 1e-300))
+    e = {f"{k}_max_rel": prof(k) for k in ("mean_u", "u_rms", "v_rms", "w_rms")}
+    for k in ("re_tau", "cf", "u_bulk", "tau_w"):
+        e[f"{k}_rel"] = abs(o[k] - ref[k]) / abs(ref[k])
+    if "slip_u_first_plane" in ref:
+        e["slip_u_rel"] = abs(o["slip_u_first_plane"] - ref["slip_u_first_plane"]) / abs(ref["slip_u_first_plane"])
+    return e
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="channel180")
+    ap.add_argument("--spinup", type=int, default=0, help="steps before the averaging window")
+    ap.add_argument("--steps", type=int, default=50000, help="steps in the averaging window")
+    ap.add_argument("--sample", type=int, default=100)
+    ap.add_argument("--precisions", default="64,64p,32,16", help="64p: FP64 control from a perturbed field")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    wl = inputs.workload(a.workload)
+    flags = inputs.make_flags(wl)
+    s0 = inputs.make_state(wl, seed=a.seed)
+    if inputs.needs_general(wl):
+        s0 = inputs.rest_solids(s0, flags)
+    runs = []
+    for p in a.precisions.split(","):
+        init = s0
+        if p == "64p":
+            rng = np.random.default_rng(a.seed + 1)
+            init = s0 * (1.0 + 1e-12 * rng.standard_normal(s0.shape))
+            if inputs.needs_general(wl):
+                init = inputs.rest_solids(init, flags)
+        try:
+            r = run_one(wl, init, flags, int(p.rstrip("p")), a.spinup, a.steps, a.sample)
+        except dnslbm.DnsLbmError as e:  # e.g. a NaN wall stress: reported, not fatal
+            r = {"failed": str(e)}
+        r["run"] = p
+        runs.append(r)
+    ref = runs[0]
+    summary = {"workload": wl.name, "grid": f"{wl.nx}x{wl.nz + 2}x{wl.ny}", "texture": wl.texture,
+               "spinup": a.spinup, "steps": a.steps, "sample_every": a.sample, "seed": a.seed, "runs": []}
+    for r in runs:
+        row = {k: v for k, v in r.items() if not isinstance(v, np.ndarray)}
+        if r is not ref and "failed" not in r and "failed" not in ref:
+            row["error_vs_fp64"] = compare(ref, r)
+        summary["runs"].append(row)
+    if "mean_u" in ref:
+        summary["fp64_mean_u_profile"] = ref["mean_u"].tolist()
+    txt = json.dumps(summary, indent=1)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(txt)
+    print(txt)
+
+
+if __name__ == "__main__":
+    main()

@@ -55,7 +55,10 @@ extern "C" {
 
 /* wall rule for solids inside the flow */
 #define DNSLBM_BC_REFERENCE 0 /* exactly xcomputations.c:359-400              */
-#define DNSLBM_BC_GENERAL 1   /* + halfway bounce-back on any no-slip link    */
+#define DNSLBM_BC_GENERAL 1   /* + solids inside the flow (riblets, blocks):  */
+                              /* bounce-back on every link into a solid cell  */
+                              /* and where a specular reflection would land   */
+                              /* on one; no counterpart in the reference      */
 
 /* per-step log record: state at the start of each step, in this order */
 #define DNSLBM_LOG_FORCE 0    /* force used by the step (V.force)               */
@@ -100,7 +103,11 @@ const char *dnslbm_last_error(const dnslbm_ctx *ctx);
  * solid_init.c:10-46, slip_ridges_init.c:3-43 and slip_posts_init.c:3-74 as
  * inputs to the step; the ghost planes are ignored (the grid is periodic). */
 int dnslbm_set_flags(dnslbm_ctx *ctx, const int *s);
-/* The same on the ghost-free periodic grid: int8 [xdv][ydv][zd]. */
+/* The same on the ghost-free periodic grid: int8 [xdv][ydv][zd].  With
+ * DNSLBM_BC_GENERAL a cell inside the flow may be solid (-1); solid cells
+ * hold the rest state f = w (a loaded state is overwritten there) and enter
+ * the plane sums like any other cell.  Wall planes are -1 or -2 in either
+ * mode; flags change only between even numbers of steps. */
 int dnslbm_set_flags_periodic(dnslbm_ctx *ctx, const int8_t *flags);
 
 /* Initial state: rest, f = w (init.c:6-19). */
@@ -157,6 +164,32 @@ int dnslbm_sync(dnslbm_ctx *ctx);
  * dns-const-q-xycut.c:248-262). */
 void *dnslbm_host_alloc(size_t bytes);
 void dnslbm_host_free(void *ptr);
+
+/* Batched channels: many independent channels (own grid, walls, force,
+ * state and logs) advanced together, one kernel launch per step for all of
+ * them, the time loop replayed from a CUDA graph in chunks of 32 steps.  All
+ * decks share one precision and device.  Use dnslbm_batch_channel(b, i) with
+ * the single-channel calls (flags, load/store, logs, statistics) between
+ * batch steps.  No counterpart in the reference (one channel per run). */
+typedef struct dnslbm_batch dnslbm_batch;
+int dnslbm_batch_create(const dnslbm_deck *decks, int n, dnslbm_batch **out);
+void dnslbm_batch_destroy(dnslbm_batch *b);
+const char *dnslbm_batch_last_error(const dnslbm_batch *b);
+int dnslbm_batch_size(const dnslbm_batch *b);
+dnslbm_ctx *dnslbm_batch_channel(dnslbm_batch *b, int i);
+/* Advance every channel nsteps steps (all channels must hold a state and be
+ * at the same step). */
+int dnslbm_batch_step(dnslbm_batch *b, long nsteps);
+/* The same, returning the device time of the whole batch in ms. */
+int dnslbm_batch_step_timed(dnslbm_batch *b, long nsteps, double *ms);
+/* Launch shape of the batched kernel. */
+const char *dnslbm_batch_kernel(const dnslbm_batch *b);
+/* Time the batched kernel's launch shapes (shared-memory budget for 1-3
+ * blocks per SM x 2-4 stages x consumer threads) on rest states of all
+ * channels, `steps` steps each, and keep the fastest.  Runs before any state
+ * is loaded (DNSLBM_ERR_STATE otherwise); leaves the channels without state.
+ * `report` (may be NULL) receives the choice. */
+int dnslbm_batch_autotune(dnslbm_batch *b, int steps, char *report, size_t report_len);
 
 /* FP64 constant-g step that allocates nothing.  No counterpart in the
  * reference: it is for callers that own all device memory through their own
