@@ -245,30 +245,30 @@ def batched_report(args, dev):
     def mode(w):
         return dnslbm.BC_GENERAL if inputs.needs_general(w) else dnslbm.BC_REFERENCE
 
-    def start(c, w):
-        fl = inputs.make_flags(w)
-        c.set_flags(fl)
-        c.load_state(inputs.rest_solids(fields[w.nz], fl) if inputs.needs_general(w) else fields[w.nz])
+    flags = [inputs.make_flags(w) for w in chans]
 
     decks = [dnslbm.deck(w.nx, w.ny, w.nz, w.omega, ubulk=w.ubulk, gx=w.gx, precision=32, bc_mode=mode(w),
                          device=dev) for w in chans]
     cells = sum(w.cells for w in chans)
     warm = max(args.warmup, 3)
     with dnslbm.Batch(decks) as b:
+        for c, fl in zip(b.channels, flags):
+            c.set_flags(fl)
         tune = None if args.no_autotune else b.autotune(8)
-        for c, w in zip(b.channels, chans):
-            start(c, w)
+        for c, w, fl in zip(b.channels, chans, flags):
+            c.load_state(inputs.rest_solids(fields[w.nz], fl) if inputs.needs_general(w) else fields[w.nz])
         b.step_timed(warm)
         ms_b = b.step_timed(args.steps)
         kdesc = b.kernel
         bpc = b.channels[0].bytes_per_cell
     ms_alone = 0.0
-    for w in chans:
+    for w, fl in zip(chans, flags):
         with dnslbm.Channel(w.nx, w.ny, w.nz, w.omega, ubulk=w.ubulk, gx=w.gx, precision=32, bc_mode=mode(w),
                             device=dev) as c:
+            c.set_flags(fl)
             if not args.no_autotune:
                 c.autotune()
-            start(c, w)
+            c.load_state(inputs.rest_solids(fields[w.nz], fl) if inputs.needs_general(w) else fields[w.nz])
             c.step_timed(warm)
             ms_alone += c.step_timed(args.steps)[0]
     peak, _ = hbm_peak()
@@ -296,12 +296,15 @@ def run_ours(args):
     cells = wl.cells
     flags = inputs.make_flags(wl)
     s0 = inputs.make_state(wl, seed=0)
+    bc = dnslbm.BC_GENERAL if inputs.needs_general(wl) else dnslbm.BC_REFERENCE
+    if inputs.needs_general(wl):
+        s0 = inputs.rest_solids(s0, flags)
     peak, peak_src = hbm_peak()
 
     ch = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, ubulk=wl.ubulk, gx=wl.gx, force_mode=dnslbm.CONST_G,
-                        precision=args.precision, device=dev)
-    tune = None if args.no_autotune else ch.autotune()
+                        precision=args.precision, bc_mode=bc, device=dev)
     ch.set_flags(flags)
+    tune = None if args.no_autotune else ch.autotune()
     ch.load_state(s0)
     ch.step_timed(args.warmup)
     d.barrier()
@@ -337,9 +340,9 @@ def run_ours(args):
         done = ch.steps_done
         for prec in (32, 16):
             c2 = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, ubulk=wl.ubulk, gx=wl.gx,
-                                force_mode=dnslbm.CONST_G, precision=prec, device=dev)
-            tune2 = None if args.no_autotune else c2.autotune()
+                                force_mode=dnslbm.CONST_G, precision=prec, bc_mode=bc, device=dev)
             c2.set_flags(flags)
+            tune2 = None if args.no_autotune else c2.autotune()
             c2.load_state(s0)
             c2.step_timed(args.warmup)
             t2, e2, o2 = c2.step_timed(args.steps)

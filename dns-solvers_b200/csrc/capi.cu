@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/dnslbm.h"
@@ -37,6 +38,8 @@ int tma_batch_prepare_lp(int precision, size_t smem);
 int tma_batch_occupancy_lp(int precision, int threads, size_t smem);
 void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem,
                          bool odd, cudaStream_t s);
+void launch_links_f64(const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s);
+void launch_links_lp(int precision, const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s);
 }  // namespace dnslbm
 
 using namespace dnslbm;
@@ -48,11 +51,18 @@ struct dnslbm_ctx {
     size_t ncell, pstride, esize;
     void *popmem = nullptr;
     uint8_t *wallmask = nullptr;
-    int textured = 0;  // 0 smooth walls, 1 textured walls, 2 solids inside the flow
+    int textured = 0;        // 0 smooth walls, 1 textured walls, 2 solids inside the flow
+    int walls_textured = 0;  // wall planes with slip cells (the row-pipelined kernel's TEX)
     int *band_of = nullptr;      // [nz] mask block of a plane next to a solid, -1: none
     unsigned *links = nullptr;   // [nband][ny][nx] per-cell link masks
     size_t links_bytes = 0;
     int nband = 0;
+    // planes of the row-pipelined kernel (nclean, ascending) followed by the
+    // planes with link masks (ndirty), which a second launch steps per cell
+    int *plane_list = nullptr;
+    int nclean = 0, ndirty = 0;
+    LinksLaunch *d_llaunch = nullptr;  // the second launch's table (one entry)
+    int tma_target = 0;                // resident blocks of the row-pipelined kernel
     double *force = nullptr, *shift = nullptr, *partials = nullptr, *plane_sums = nullptr, *logs = nullptr;
     long long *step_ctr = nullptr, *status = nullptr;
     unsigned *plane_ctr = nullptr, *total_ctr = nullptr;
@@ -60,6 +70,8 @@ struct dnslbm_ctx {
     size_t staging_bytes = 0;
     double *stat_partials = nullptr, *stat_planes = nullptr, *stat_mean = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;                // the per-cell pass runs here beside the bulk kernel
+    cudaEvent_t fj[2] = {nullptr, nullptr};     // fork / join of the side stream
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> tev;  // per-launch timing events
     dim3 grid, block;
@@ -67,7 +79,7 @@ struct dnslbm_ctx {
     int slots = 1;  // partial-sum slots per plane
     // row-pipelined (bulk-copy) step
     int use_tma = 0, tma_threads = 0, tma_grid = 0;
-    char kernel_desc[160] = {0};
+    char kernel_desc[256] = {0};
     size_t tma_smem = 0;
     TmaArgs tma{};
     int have_state = 0;
@@ -142,14 +154,19 @@ static IoArgs io_args(const dnslbm_ctx *c)
 
 static void free_all(dnslbm_ctx *c)
 {
-    void *ptrs[] = {c->popmem, c->wallmask, c->force, c->shift, c->partials, c->plane_sums, c->logs, c->step_ctr,
-                    c->status, c->plane_ctr, c->total_ctr, c->staging, c->stat_partials, c->stat_planes, c->stat_mean, c->band_of, c->links};
+    void *ptrs[] = {c->popmem,     c->wallmask,   c->force,         c->shift,       c->partials,
+                    c->plane_sums, c->logs,       c->step_ctr,      c->status,      c->plane_ctr,
+                    c->total_ctr,  c->staging,    c->stat_partials, c->stat_planes, c->stat_mean,
+                    c->band_of,    c->links,      c->plane_list,    c->d_llaunch};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : c->tev)
         if (e) cudaEventDestroy(e);
+    for (auto &e : c->fj)
+        if (e) cudaEventDestroy(e);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -159,6 +176,19 @@ extern "C" const char *dnslbm_last_error(const dnslbm_ctx *c) { return c ? c->er
 // groups in flight and `consumers` compute threads (+ one producer warp);
 // bps > 0 caps the blocks per SM.  Returns 0 when the configuration runs on
 // this device (and selects it), -1 otherwise (the previous choice stays).
+// Row groups of the row-pipelined kernel over its planes (all planes, or the
+// planes without link masks) shared among tma_target blocks.
+static void tma_layout(dnslbm_ctx *c)
+{
+    const int ngroups = c->tma.gpp * c->nclean;
+    const int target = std::max(1, c->tma_target);
+    const int GB = std::max(1, (ngroups + target - 1) / target);
+    c->tma.ngroups = ngroups;
+    c->tma.groups_per_block = GB;
+    c->tma.planes = c->nclean < c->nz ? c->plane_list : nullptr;
+    c->tma_grid = (ngroups + GB - 1) / GB;
+}
+
 static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bps)
 {
     const int row_bytes = c->pitch * (int)c->esize;
@@ -178,29 +208,44 @@ static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bp
     cudaGetLastError();  // a failed query only rules the configuration out
     if (bps > 0) occ = std::min(occ, bps);
     if (occ < 1) return -1;
-    const int gpp = (c->ny + k - 1) / k, ngroups = gpp * c->nz;
-    const int target = occ * nsm;
-    const int GB = (ngroups + target - 1) / target;
+    const int gpp = (c->ny + k - 1) / k;
     c->use_tma = 1;
     c->tma_threads = threads;
     c->tma_smem = smem;
-    c->tma_grid = (ngroups + GB - 1) / GB;
-    c->tma = TmaArgs{ngroups, GB, stages, row_bytes, k, gpp};
+    c->tma_target = occ * nsm;
+    c->tma = TmaArgs{0, 1, stages, row_bytes, k, gpp, nullptr};
+    tma_layout(c);
     return 0;
 }
 
 static void describe_kernel(dnslbm_ctx *c)
 {
-    if (c->use_tma)
-        snprintf(c->kernel_desc, sizeof c->kernel_desc,
-                 "step_tma_kernel<fp%d> row-pipelined bulk-copy: %d blocks x %d threads, %d groups of %d rows/block, "
-                 "%d stages, %zu B smem",
-                 c->deck.precision, c->tma_grid, c->tma_threads, c->tma.groups_per_block, c->tma.k, c->tma.stages,
-                 c->tma_smem);
-    else
+    if (c->use_tma) {
+        int m = snprintf(c->kernel_desc, sizeof c->kernel_desc,
+                         "step_tma_kernel<fp%d> row-pipelined bulk-copy: %d blocks x %d threads, %d groups of %d "
+                         "rows/block, %d stages, %zu B smem",
+                         c->deck.precision, c->tma_grid, c->tma_threads, c->tma.groups_per_block, c->tma.k,
+                         c->tma.stages, c->tma_smem);
+        if (c->ndirty > 0 && m > 0 && m < (int)sizeof c->kernel_desc)
+            snprintf(c->kernel_desc + m, sizeof c->kernel_desc - m, " + links_pass_kernel over %d planes", c->ndirty);
+    } else {
         snprintf(c->kernel_desc, sizeof c->kernel_desc, "%s per-thread: grid %ux%ux%u x %u threads",
                  c->deck.precision == 64 ? "step_f64_kernel" : "step_lp_kernel", c->grid.x, c->grid.y, c->grid.z,
                  c->block.x);
+    }
+}
+
+// plane_list: the planes without link masks, then those with them
+static cudaError_t upload_planes(dnslbm_ctx *c, const std::vector<int> *band = nullptr)
+{
+    std::vector<int> pl;
+    for (int z = 0; z < c->nz; ++z)
+        if (!band || (*band)[z] < 0) pl.push_back(z);
+    c->nclean = (int)pl.size();
+    for (int z = 0; z < c->nz; ++z)
+        if (band && (*band)[z] >= 0) pl.push_back(z);
+    c->ndirty = c->nz - c->nclean;
+    return cudaMemcpy(c->plane_list, pl.data(), pl.size() * sizeof(int), cudaMemcpyHostToDevice);
 }
 
 extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
@@ -228,6 +273,7 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     c->nx = deck->xdv;
     c->ny = deck->ydv;
     c->nz = deck->zdv;
+    c->nclean = c->nz;
     c->esize = deck->precision / 8;
     {
         // rows start on `align` bytes (16 at least, for the bulk copies)
@@ -307,6 +353,8 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         {(void **)&c->stat_planes, (size_t)c->nz * 5 * sizeof(double)},
         {(void **)&c->stat_mean, (size_t)c->nz * 4 * sizeof(double)},
         {(void **)&c->band_of, (size_t)c->nz * sizeof(int)},
+        {(void **)&c->plane_list, (size_t)c->nz * sizeof(int)},
+        {(void **)&c->d_llaunch, sizeof(LinksLaunch)},
     };
     for (auto &a : al) {
         cudaError_t e = cudaMalloc(a.p, a.bytes);
@@ -316,8 +364,11 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         }
         cudaMemset(*a.p, 0, a.bytes);
     }
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        fail(c, DNSLBM_ERR_CUDA, "cannot create stream");
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->fj[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->fj[1], cudaEventDisableTiming) != cudaSuccess) {
+        fail(c, DNSLBM_ERR_CUDA, "cannot create streams");
         return bail(DNSLBM_ERR_CUDA);
     }
     for (auto &e : c->ev)
@@ -329,6 +380,7 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     std::vector<uint8_t> m((size_t)2 * c->nx * c->ny, 0x1f);
     if (cudaMemcpy(c->wallmask, m.data(), m.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(c->band_of, 0xff, (size_t)c->nz * sizeof(int)) != cudaSuccess ||
+        upload_planes(c) != cudaSuccess ||
         cudaDeviceSynchronize() != cudaSuccess) {
         fail(c, DNSLBM_ERR_CUDA, "initialisation failed: %s", cudaGetErrorString(cudaGetLastError()));
         return bail(DNSLBM_ERR_CUDA);
@@ -452,8 +504,24 @@ static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
     CK(cudaMemcpyAsync(c->band_of, band.data(), band.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     if (lbytes) CK(cudaMemcpyAsync(c->links, lk.data(), lbytes, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    c->walls_textured = 0;
+    for (size_t i = 0; i < m.size() && !c->walls_textured; ++i) c->walls_textured = m[i] != 0x1f;
     c->textured = textured;
     c->nband = nband;
+    CK(upload_planes(c, &band));
+    {
+        LinksLaunch L{};
+        L.p = step_args(c);
+        L.planes = c->plane_list + c->nclean;
+        L.nplanes = c->ndirty;
+        L.xblocks = (int)c->grid.x;
+        L.yblocks = (int)c->grid.y;
+        L.rows = c->rows;
+        L.first_block = 0;
+        CK(cudaMemcpy(c->d_llaunch, &L, sizeof L, cudaMemcpyHostToDevice));
+    }
+    if (c->use_tma) tma_layout(c);
+    describe_kernel(c);
     if (textured == 2 && c->have_state) {
         // cells that became solid take the rest state; the sums of the
         // current step are taken again
@@ -575,11 +643,32 @@ static int launch_steps(dnslbm_ctx *c, long n, bool timed, double *ms_even, doub
         const bool odd = c->odd != 0;
         if (timed) CK(cudaEventRecord(c->tev[2 * s], c->stream));
         if (c->use_tma) {
-            if (c->deck.precision == 64)
-                launch_tma_f64(p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd, c->textured, c->stream);
-            else
-                launch_tma_lp(c->deck.precision, p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd,
-                              c->textured, c->stream);
+            // the row-pipelined kernel over its planes and, beside it on a
+            // second stream, the planes with link masks per cell (disjoint
+            // addresses; whichever finishes the last plane runs the step tail)
+            const bool both = c->tma.ngroups > 0 && c->ndirty > 0;
+            cudaStream_t ls = both ? c->side : c->stream;
+            if (both) {
+                CK(cudaEventRecord(c->fj[0], c->stream));
+                CK(cudaStreamWaitEvent(c->side, c->fj[0], 0));
+            }
+            if (c->tma.ngroups > 0) {
+                if (c->deck.precision == 64)
+                    launch_tma_f64(p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd, c->walls_textured,
+                                   c->stream);
+                else
+                    launch_tma_lp(c->deck.precision, p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd,
+                                  c->walls_textured, c->stream);
+            }
+            if (c->ndirty > 0) {
+                const int blocks = c->ndirty * (int)(c->grid.x * c->grid.y);
+                if (c->deck.precision == 64) launch_links_f64(c->d_llaunch, 1, blocks, odd, ls);
+                else launch_links_lp(c->deck.precision, c->d_llaunch, 1, blocks, odd, ls);
+            }
+            if (both) {
+                CK(cudaEventRecord(c->fj[1], c->side));
+                CK(cudaStreamWaitEvent(c->stream, c->fj[1], 0));
+            }
         } else if (c->deck.precision == 64) {
             launch_step_f64(p, c->grid, c->block, odd, c->textured, c->stream);
         } else {
@@ -767,17 +856,21 @@ extern "C" void dnslbm_host_free(void *p)
 
 // ---------------------------------------------------------------- autotuner
 struct TmaChoice {
-    int use_tma, threads, grid;
+    int use_tma, threads, grid, target;
     size_t smem;
     TmaArgs t;
 };
 
-static TmaChoice save_choice(const dnslbm_ctx *c) { return {c->use_tma, c->tma_threads, c->tma_grid, c->tma_smem, c->tma}; }
+static TmaChoice save_choice(const dnslbm_ctx *c)
+{
+    return {c->use_tma, c->tma_threads, c->tma_grid, c->tma_target, c->tma_smem, c->tma};
+}
 static void load_choice(dnslbm_ctx *c, const TmaChoice &k)
 {
     c->use_tma = k.use_tma;
     c->tma_threads = k.threads;
     c->tma_grid = k.grid;
+    c->tma_target = k.target;
     c->tma_smem = k.smem;
     c->tma = k.t;
 }
@@ -856,6 +949,9 @@ struct dnslbm_batch {
     int precision = 64, device = 0;
     cudaStream_t stream = nullptr;
     ChannelLaunch *d_launch = nullptr;
+    LinksLaunch *d_links = nullptr;  // channels with planes next to solids
+    int nlinks = 0, links_blocks = 0;
+    int target = 0;                  // resident blocks of the row-pipelined kernel
     int grid = 0, threads = 0;
     size_t smem = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // a chunk of steps starting on an even / odd parity
@@ -863,6 +959,8 @@ struct dnslbm_batch {
     size_t budget = 0;  // shared-memory budget per block the stages were sized for
     int stages = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaStream_t side = nullptr;             // the per-cell pass beside the bulk kernel
+    cudaEvent_t fj[2] = {nullptr, nullptr};  // fork / join of the side stream
     char err[512] = {0};
 };
 
@@ -902,6 +1000,10 @@ extern "C" void dnslbm_batch_destroy(dnslbm_batch *b)
     for (auto &e : b->ev)
         if (e) cudaEventDestroy(e);
     if (b->d_launch) cudaFree(b->d_launch);
+    if (b->d_links) cudaFree(b->d_links);
+    for (auto &e : b->fj)
+        if (e) cudaEventDestroy(e);
+    if (b->side) cudaStreamDestroy(b->side);
     if (b->stream) cudaStreamDestroy(b->stream);
     for (auto *c : b->ch) dnslbm_destroy(c);
     delete b;
@@ -912,16 +1014,61 @@ extern "C" void dnslbm_batch_destroy(dnslbm_batch *b)
 // the kernel on top).
 constexpr size_t kBatchBudget1 = 220 * 1024, kBatchBudget2 = 108 * 1024, kBatchBudget3 = 70 * 1024;
 
+// Row groups of every channel's planes without link masks shared among the
+// resident blocks, each block taking whole row groups of one channel and
+// about the same number of cells, and the block count of the per-cell pass
+// over the planes with link masks.  A change of
+// either grid invalidates the captured graphs.
+static void batch_layout(dnslbm_batch *b)
+{
+    // a common amount of work per block (cells of whole row groups), the
+    // smallest for which the blocks fit the resident set at once
+    double total = 0;
+    for (auto *c : b->ch) total += (double)c->nx * c->ny * c->nclean;
+    const int target = std::max(1, b->target);
+    auto blocks_for = [&](double w, dnslbm_ctx *c) {
+        const double cells = (double)c->nx * c->ny * c->nclean;
+        if (cells <= 0) return 0;
+        const int ng = c->tma.gpp * c->nclean;
+        const int want = std::max(1, std::min(ng, (int)std::ceil(cells / w)));
+        const int gpb = (ng + want - 1) / want;
+        return (ng + gpb - 1) / gpb;
+    };
+    double w = std::max(1.0, total / target);
+    for (int it = 0; it < 400; ++it, w *= 1.01) {
+        int sum = 0;
+        for (auto *c : b->ch) sum += blocks_for(w, c);
+        if (sum <= target) break;
+    }
+    int grid = 0, lblocks = 0, nl = 0;
+    for (auto *c : b->ch) {
+        TmaArgs &t = c->tma;
+        t.ngroups = t.gpp * c->nclean;
+        t.planes = c->nclean < c->nz ? c->plane_list : nullptr;
+        const int nb = blocks_for(w, c);
+        t.groups_per_block = nb > 0 ? (t.ngroups + nb - 1) / nb : 1;
+        c->tma_grid = nb;
+        grid += c->tma_grid;
+        if (c->ndirty > 0) {
+            lblocks += c->ndirty * (int)(c->grid.x * c->grid.y);
+            ++nl;
+        }
+    }
+    if (grid != b->grid || lblocks != b->links_blocks) destroy_graphs(b);
+    b->grid = grid;
+    b->links_blocks = lblocks;
+    b->nlinks = nl;
+}
+
 // One launch shape for all channels: per channel the most rows per stage
 // group (1, 2, 4 or 8) whose `stages` groups fit `budget` bytes; the block
-// takes the largest of these; blocks are shared among the channels in
-// proportion to their cells.  Returns 0 and selects the shape when it runs
+// takes the largest of these.  Returns 0 and selects the shape when it runs
 // on the device.
 static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consumers)
 {
     consumers = std::max(32, std::min(352, consumers / 32 * 32));
     size_t smem = 0;
-    std::vector<TmaArgs> t(b->ch.size());
+    std::vector<int> ks(b->ch.size());
     for (size_t i = 0; i < b->ch.size(); ++i) {
         dnslbm_ctx *c = b->ch[i];
         const int row_bytes = c->pitch * (int)c->esize;
@@ -929,8 +1076,7 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
         if (need(1) > budget) return -1;
         int k = 1;
         while (k < 8 && 2 * k <= c->ny && need(2 * k) <= budget) k *= 2;
-        const int gpp = (c->ny + k - 1) / k;
-        t[i] = TmaArgs{gpp * c->nz, 1, stages, row_bytes, k, gpp};
+        ks[i] = k;
         smem = std::max(smem, need(k));
     }
     const int threads = consumers + 32;
@@ -942,27 +1088,21 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
     if (occ < 1 || nsm < 1) return -1;
-    double total = 0;
-    for (auto *c : b->ch) total += (double)c->nx * c->ny * c->nz;
-    const int target = occ * nsm;
-    int grid = 0;
     for (size_t i = 0; i < b->ch.size(); ++i) {
         dnslbm_ctx *c = b->ch[i];
-        const double share = (double)c->nx * c->ny * c->nz / total;
-        const int want = std::max(1, (int)(target * share + 0.5));
-        t[i].groups_per_block = (t[i].ngroups + want - 1) / want;
-        c->tma = t[i];
-        c->tma_grid = (t[i].ngroups + t[i].groups_per_block - 1) / t[i].groups_per_block;
+        const int row_bytes = c->pitch * (int)c->esize;
+        c->tma = TmaArgs{0, 1, stages, row_bytes, ks[i], (c->ny + ks[i] - 1) / ks[i], nullptr};
         c->tma_threads = threads;
         c->tma_smem = smem;
-        grid += c->tma_grid;
+        c->tma_target = occ * nsm;
     }
-    b->grid = grid;
+    b->target = occ * nsm;
     b->threads = threads;
     b->smem = smem;
     b->budget = budget;
     b->stages = stages;
     destroy_graphs(b);
+    batch_layout(b);
     return 0;
 }
 
@@ -1009,7 +1149,11 @@ extern "C" int dnslbm_batch_create(const dnslbm_deck *decks, int n, dnslbm_batch
         return bail(bfail(b, DNSLBM_ERR_ARG, "batched kernel does not fit the device"));
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess ||
-        cudaMalloc(&b->d_launch, sizeof(ChannelLaunch) * n) != cudaSuccess)
+        cudaMalloc(&b->d_launch, sizeof(ChannelLaunch) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_links, sizeof(LinksLaunch) * n) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fj[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fj[1], cudaEventDisableTiming) != cudaSuccess)
         return bail(bfail(b, DNSLBM_ERR_CUDA, "batch set-up failed: %s", cudaGetErrorString(cudaGetLastError())));
     *out = b;
     return DNSLBM_OK;
@@ -1023,11 +1167,28 @@ extern "C" dnslbm_ctx *dnslbm_batch_channel(dnslbm_batch *b, int i)
 
 static int batch_launch(dnslbm_batch *b, bool odd)
 {
-    if (b->precision == 64)
-        launch_tma_batch_f64(b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd, b->stream);
-    else
-        launch_tma_batch_lp(b->precision, b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd,
-                            b->stream);
+    // the bulk kernel and, beside it on a second stream, the per-cell pass
+    const bool both = b->grid > 0 && b->links_blocks > 0;
+    cudaStream_t ls = both ? b->side : b->stream;
+    if (both) {
+        BCK(cudaEventRecord(b->fj[0], b->stream));
+        BCK(cudaStreamWaitEvent(b->side, b->fj[0], 0));
+    }
+    if (b->grid > 0) {
+        if (b->precision == 64)
+            launch_tma_batch_f64(b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd, b->stream);
+        else
+            launch_tma_batch_lp(b->precision, b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd,
+                                b->stream);
+    }
+    if (b->links_blocks > 0) {
+        if (b->precision == 64) launch_links_f64(b->d_links, b->nlinks, b->links_blocks, odd, ls);
+        else launch_links_lp(b->precision, b->d_links, b->nlinks, b->links_blocks, odd, ls);
+    }
+    if (both) {
+        BCK(cudaEventRecord(b->fj[1], b->side));
+        BCK(cudaStreamWaitEvent(b->stream, b->fj[1], 0));
+    }
     BCK(cudaGetLastError());
     return DNSLBM_OK;
 }
@@ -1044,18 +1205,35 @@ static int batch_run(dnslbm_batch *b, long nsteps, double *ms)
         if (c->stream) BCK(cudaStreamSynchronize(c->stream));
     }
     BCK(cudaSetDevice(b->device));
-    // launch table (flags may have changed a channel's wall mode)
+    // launch tables (flags may have changed a channel's walls and planes)
+    batch_layout(b);
     std::vector<ChannelLaunch> h(n);
-    int first = 0;
+    std::vector<LinksLaunch> hl;
+    int first = 0, lfirst = 0;
     for (int i = 0; i < n; ++i) {
         dnslbm_ctx *c = b->ch[i];
         h[i].p = step_args(c);
         h[i].t = c->tma;
         h[i].first_block = first;
-        h[i].textured = c->textured;
+        h[i].textured = c->walls_textured;
         first += c->tma_grid;
+        if (c->ndirty > 0) {
+            LinksLaunch L{};
+            L.p = h[i].p;
+            L.planes = c->plane_list + c->nclean;
+            L.nplanes = c->ndirty;
+            L.xblocks = (int)c->grid.x;
+            L.yblocks = (int)c->grid.y;
+            L.rows = c->rows;
+            L.first_block = lfirst;
+            lfirst += c->ndirty * L.xblocks * L.yblocks;
+            hl.push_back(L);
+        }
     }
     BCK(cudaMemcpyAsync(b->d_launch, h.data(), sizeof(ChannelLaunch) * n, cudaMemcpyHostToDevice, b->stream));
+    if (!hl.empty())
+        BCK(cudaMemcpyAsync(b->d_links, hl.data(), sizeof(LinksLaunch) * hl.size(), cudaMemcpyHostToDevice,
+                            b->stream));
     int odd = b->ch[0]->odd;
     long left = nsteps;
     if (ms) BCK(cudaEventRecord(b->ev[0], b->stream));
@@ -1118,9 +1296,10 @@ extern "C" const char *dnslbm_batch_kernel(const dnslbm_batch *b)
 {
     static thread_local char buf[256];
     if (!b) return "";
-    snprintf(buf, sizeof buf, "step_tma_batch_kernel<fp%d>: %zu channels, %d blocks x %d threads, %d stages, %zu B smem, "
-             "CUDA graph of %d steps", b->precision, b->ch.size(), b->grid, b->threads, b->stages, b->smem,
-             b->graph_steps);
+    snprintf(buf, sizeof buf, "step_tma_batch_kernel<fp%d>: %zu channels, %d blocks x %d threads, %d stages, %zu B smem"
+             "%s%s; CUDA graph of %d steps", b->precision, b->ch.size(), b->grid, b->threads, b->stages, b->smem,
+             b->links_blocks ? " + links_pass_kernel: " : "",
+             b->links_blocks ? (std::to_string(b->links_blocks) + " blocks").c_str() : "", b->graph_steps);
     return buf;
 }
 

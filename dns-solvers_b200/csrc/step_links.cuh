@@ -1,12 +1,14 @@
 // Cells of the planes next to solids inside the flow (boundary mode
 // DNSLBM_BC_GENERAL: riblets, bars, blocks).  Such a plane carries a per-cell
 // link mask (cell_links, step_common.cuh) and its cells move every
-// population by a per-thread access in an odd step, because a bounced link's
-// address is a slot of the cell's own row that the bulk row of another
-// direction would also cover.  Solid cells are never collided: they keep the
-// rest state, and their stored populations enter the plane sums as they are,
-// so the sums run over every cell of the plane like the reference's encalc /
-// wshearstr / statistics loops.
+// population by a per-thread access: a bounced link's address is a slot of
+// the cell's own row that the bulk row of another direction would also
+// cover, so these planes are left out of the row-pipelined kernel and
+// stepped by links_pass_kernel (below) right after it, or by the per-thread
+// step kernels.  Solid cells are never collided: they keep the rest state,
+// and their stored populations enter the plane sums as they are, so the sums
+// run over every cell of the plane like the reference's encalc / wshearstr /
+// statistics loops.
 #pragma once
 
 #include <type_traits>
@@ -211,6 +213,84 @@ __device__ __forceinline__ void links_cell(const StepArgs &p, const Nbr &n, int 
         else if (!ODD) st_raw<T>(static_cast<T *>(p.pop[A]) + n.c0, v);
         else st_raw<T>(links_ptr<T, A>(p, n, wall, lk), v);
     });
+}
+
+// ------------------------------------------------------------------ pass
+// The planes with link masks of one or more channels, one thread per x and
+// `rows` rows per block (the per-thread kernels' block shape, so a plane has
+// as many contributors as there are partial-sum slots).  It runs as the
+// second launch of a step, after the row-pipelined kernel has done the
+// other planes; the last plane to finish runs the step tail.
+struct LinksLaunch {
+    StepArgs p;
+    const int *planes;  // the channel's planes with link masks
+    int nplanes;
+    int xblocks, yblocks, rows;
+    int first_block;    // first block of the channel in the launch
+};
+
+template <typename T, bool ODD, bool CONSTQ>
+__device__ __forceinline__ void links_pass_body(const LinksLaunch &L, int blk)
+{
+    const StepArgs &p = L.p;
+    const int per_plane = L.xblocks * L.yblocks;
+    const int pi = blk / per_plane, r = blk - pi * per_plane;
+    const int by = r / L.xblocks, bx = r - by * L.xblocks;
+    const int z = L.planes[pi];
+    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const long long step = *p.step_ctr;
+    const double G = CONSTQ ? p.force[step & 1] : p.gx;
+    const double *sh = p.shift + (size_t)(step & 1) * p.nz * 3 + z * 3;
+    const double c0 = sh[0], c1 = sh[1], c2 = sh[2];
+    double acc[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) acc[i] = 0.0;
+    const int x = bx * blockDim.x + threadIdx.x;
+    if (x < p.nx) {
+        const int y0 = by * L.rows, y1 = min(y0 + L.rows, p.ny);
+        for (int y = y0; y < y1; ++y) {
+            float racc[NP];
+#pragma unroll
+            for (int i = 0; i < NP; ++i) racc[i] = 0.f;
+            const Nbr n = make_nbr(x, y, z, p.nx, p.ny, p.pitch);
+            links_cell<T, ODD, CONSTQ>(p, n, wall, cell_links(p.band_of, p.links, p.nx, p.ny, x, y, z), nullptr, 0,
+                                       G, c0, c1, c2, acc, racc);
+#pragma unroll
+            for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i];
+        }
+    }
+    plane_contribute(p, acc, z, r, per_plane, step, G, 0, blockDim.x);
+}
+
+constexpr int kLinksThreads = 128;
+
+template <typename T, bool ODD>
+__global__ void __launch_bounds__(kLinksThreads) links_pass_kernel(const LinksLaunch *__restrict__ tab, int n)
+{
+    __shared__ LinksLaunch L;
+    __shared__ int s_c;
+    if (threadIdx.x == 0) {
+        int c = 0;
+        while (c + 1 < n && tab[c + 1].first_block <= (int)blockIdx.x) ++c;
+        s_c = c;
+    }
+    __syncthreads();
+    {
+        const int *src = reinterpret_cast<const int *>(tab + s_c);
+        int *dst = reinterpret_cast<int *>(&L);
+        for (int i = threadIdx.x; i < (int)(sizeof(LinksLaunch) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const int blk = blockIdx.x - L.first_block;
+    if (L.p.const_q) links_pass_body<T, ODD, true>(L, blk);
+    else links_pass_body<T, ODD, false>(L, blk);
+}
+
+template <typename T>
+void launch_links_pass(const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s)
+{
+    if (odd) links_pass_kernel<T, true><<<blocks, kLinksThreads, 0, s>>>(tab, n);
+    else links_pass_kernel<T, false><<<blocks, kLinksThreads, 0, s>>>(tab, n);
 }
 
 }  // namespace dnslbm

@@ -24,10 +24,10 @@
 // textured wall the five links into the wall go to rows that several cell
 // rows share (bounce-back or specular per cell), so those five are moved by
 // per-thread loads/stores and never by a bulk copy.  Planes next to solids
-// inside the flow (TEX 2) move all 19 per thread in an odd step
-// (step_links.cuh); their even step is bulk like any other.
+// inside the flow are not in this kernel's plane list: a second launch of
+// the same step (links_pass_kernel, step_links.cuh) moves them per thread.
 //
-// TEX: 0 smooth walls, 1 textured walls, 2 solids inside the flow.
+// TEX: 0 smooth walls, 1 textured walls.
 //
 // Every wait on an mbarrier is bounded; a wait that runs out records
 // status[1] and a shared abort flag, after which no thread of the block waits
@@ -52,7 +52,16 @@ struct TmaArgs {
     int row_bytes;        // pitch * sizeof(storage)
     int k;                // cell rows per group (consecutive y of one plane)
     int gpp;              // groups per plane, ceil(ny / k)
+    const int *planes;    // planes of the kernel's groups in order (nullptr: 0 .. nz-1)
 };
+
+// Plane and first row of row group gi.
+__device__ __forceinline__ void group_origin(const TmaArgs &t, int gi, int &z, int &y0)
+{
+    const int pi = gi / t.gpp;
+    z = t.planes ? t.planes[pi] : pi;
+    y0 = (gi - pi * t.gpp) * t.k;
+}
 
 // ------------------------------------------------------------------ PTX
 __device__ __forceinline__ uint32_t sm_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -130,9 +139,6 @@ __device__ __forceinline__ GroupRows group_rows(const StepArgs &p, int A, int y0
     const int ez = lat_ez(A);
     g.bulk = true;
     if (!ODD) {
-        g.slot = A; g.zz = z; g.y_first = y0;
-    } else if (TEX == 2 && p.band_of[z] >= 0) {
-        g.bulk = false;  // plane next to a solid: every link per thread
         g.slot = A; g.zz = z; g.y_first = y0;
     } else if (ez != 0 && ez == wall) {
         g.bulk = TEX == 0;
@@ -292,27 +298,6 @@ __device__ __forceinline__ void tma_row(const StepArgs &p, T *sb, int dstride, i
     }
 }
 
-// One cell row of a plane next to a solid (TEX 2): per-cell link masks.
-template <typename T, bool ODD, bool CONSTQ>
-__device__ __forceinline__ void links_row(const StepArgs &p, T *sb, int dstride, int y, int z, double G,
-                                          const double *shift, double (&acc)[NP], int nc)
-{
-    const int nx = p.nx, wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
-    const unsigned *lrow = p.links + ((size_t)p.band_of[z] * p.ny + y) * nx;
-    float racc[NP];
-#pragma unroll
-    for (int i = 0; i < NP; ++i) racc[i] = 0.f;
-    for (int x = threadIdx.x; x < nx; x += nc) {
-        const Nbr n = make_nbr(x, y, z, nx, p.ny, p.pitch);
-        links_cell<T, ODD, CONSTQ>(p, n, wall, lrow[x], ODD ? nullptr : sb + x, dstride, G, shift[0], shift[1],
-                                   shift[2], acc, racc);
-    }
-    if constexpr (!std::is_same<T, double>::value) {
-#pragma unroll
-        for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i];
-    }
-}
-
 // ------------------------------------------------------------------ kernel
 // Producer warp: lane A < 19 moves direction A's rows of every row group of
 // the block; lane 0 also arms the stage's full barrier with the byte count.
@@ -330,7 +315,9 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
                 *abort = 1;
                 atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
             }
-            const int gi = g0 + i - S, z = gi / t.gpp, y0 = (gi - z * t.gpp) * t.k;
+            const int gi = g0 + i - S;
+            int z, y0;
+            group_origin(t, gi, z, y0);
             const int k = min(t.k, p.ny - y0);
             const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
             if (lane < Q && !*abort) {
@@ -340,7 +327,9 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             }
         }
         if (i < n) {  // load group i into the stage
-            const int gi = g0 + i, z = gi / t.gpp, y0 = (gi - z * t.gpp) * t.k;
+            const int gi = g0 + i;
+            int z, y0;
+            group_origin(t, gi, z, y0);
             const int k = min(t.k, p.ny - y0);
             const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
             GroupRows g{};
@@ -396,7 +385,8 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
     for (int i = 0; i < NP; ++i) acc[i] = 0.0;
     for (int i = 0; i < n; ++i) {
         const int st = i % S, gi = g0 + i;
-        const int z = gi / t.gpp, y0 = (gi - z * t.gpp) * t.k;
+        int z, y0;
+        group_origin(t, gi, z, y0);
         const int k = min(t.k, p.ny - y0);
         if (!*(volatile int *)&s_abort && !mbar_wait_bounded(full + st, (uint32_t)((i / S) & 1))) {
             s_abort = 1;
@@ -405,11 +395,9 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
         T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
         const double *sh = shift_now + z * 3;
         constexpr bool TXT = TEX != 0;
-        const bool links = TEX == 2 && p.band_of[z] >= 0;
         for (int j = 0; j < k; ++j) {
             T *sbj = sb + (size_t)j * p.pitch;
-            if (links) links_row<T, ODD, CONSTQ>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
-            else if (z == 0) tma_row<T, ODD, CONSTQ, TXT, -1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
+            if (z == 0) tma_row<T, ODD, CONSTQ, TXT, -1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
             else if (z == p.nz - 1) tma_row<T, ODD, CONSTQ, TXT, 1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
             else tma_row<T, ODD, CONSTQ, TXT, 0>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
         }
@@ -417,8 +405,9 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);
         if (i + 1 == n || (gi + 1) % t.gpp == 0) {  // this block's last group of plane z
-            const int bfirst = (z * t.gpp) / G_;
-            const int blast = min(((z + 1) * t.gpp - 1) / G_, (t.ngroups - 1) / G_);
+            const int pi = gi / t.gpp;  // position of plane z in the kernel's plane list
+            const int bfirst = (pi * t.gpp) / G_;
+            const int blast = min(((pi + 1) * t.gpp - 1) / G_, (t.ngroups - 1) / G_);
             plane_contribute(p, acc, z, blk - bfirst, blast - bfirst + 1, step, G, 0, nc);
 #pragma unroll
             for (int q = 0; q < NP; ++q) acc[q] = 0.0;
@@ -440,7 +429,7 @@ struct ChannelLaunch {
     StepArgs p;
     TmaArgs t;
     int first_block;
-    int textured;  // TEX of the channel
+    int textured;  // TEX of the channel (0 smooth, else textured walls)
 };
 
 template <typename T, bool ODD>
@@ -465,12 +454,10 @@ __global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_batch_kernel(const
     const int blk = blockIdx.x - L.first_block;
     const bool q = L.p.const_q != 0;
     if (q) {
-        if (L.textured == 2) tma_step_body<T, ODD, true, 2>(L.p, L.t, blk, tma_smem);
-        else if (L.textured) tma_step_body<T, ODD, true, 1>(L.p, L.t, blk, tma_smem);
+        if (L.textured) tma_step_body<T, ODD, true, 1>(L.p, L.t, blk, tma_smem);
         else tma_step_body<T, ODD, true, 0>(L.p, L.t, blk, tma_smem);
     } else {
-        if (L.textured == 2) tma_step_body<T, ODD, false, 2>(L.p, L.t, blk, tma_smem);
-        else if (L.textured) tma_step_body<T, ODD, false, 1>(L.p, L.t, blk, tma_smem);
+        if (L.textured) tma_step_body<T, ODD, false, 1>(L.p, L.t, blk, tma_smem);
         else tma_step_body<T, ODD, false, 0>(L.p, L.t, blk, tma_smem);
     }
 }
@@ -480,11 +467,9 @@ int tma_set_smem_attr(size_t bytes)
 {
     const void *ks[] = {
         (const void *)step_tma_kernel<T, false, false, 0>, (const void *)step_tma_kernel<T, false, false, 1>,
-        (const void *)step_tma_kernel<T, false, false, 2>, (const void *)step_tma_kernel<T, false, true, 0>,
-        (const void *)step_tma_kernel<T, false, true, 1>,  (const void *)step_tma_kernel<T, false, true, 2>,
+        (const void *)step_tma_kernel<T, false, true, 0>,  (const void *)step_tma_kernel<T, false, true, 1>,
         (const void *)step_tma_kernel<T, true, false, 0>,  (const void *)step_tma_kernel<T, true, false, 1>,
-        (const void *)step_tma_kernel<T, true, false, 2>,  (const void *)step_tma_kernel<T, true, true, 0>,
-        (const void *)step_tma_kernel<T, true, true, 1>,   (const void *)step_tma_kernel<T, true, true, 2>};
+        (const void *)step_tma_kernel<T, true, true, 0>,   (const void *)step_tma_kernel<T, true, true, 1>};
     for (const void *k : ks)
         if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return -1;
     return 0;
@@ -506,7 +491,7 @@ void launch_tma(const StepArgs &p, const TmaArgs &t, int grid, int threads, size
 {
     const bool q = p.const_q != 0;
 #define L(O, C, X) step_tma_kernel<T, O, C, X><<<grid, threads, smem, s>>>(p, t)
-#define LX(O, C) do { if (tex == 2) L(O, C, 2); else if (tex) L(O, C, 1); else L(O, C, 0); } while (0)
+#define LX(O, C) do { if (tex) L(O, C, 1); else L(O, C, 0); } while (0)
     if (odd) {
         if (q) LX(true, true); else LX(true, false);
     } else {

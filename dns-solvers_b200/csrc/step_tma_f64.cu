@@ -20,4 +20,10 @@ void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, int grid, int t
     launch_tma_batch<double>(chans, nchan, grid, threads, smem, odd, s);
 }
 
+
+void launch_links_f64(const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s)
+{
+    launch_links_pass<double>(tab, n, blocks, odd, s);
+}
+
 }  // namespace dnslbm

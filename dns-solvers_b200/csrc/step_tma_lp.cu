@@ -33,4 +33,11 @@ void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, i
     else launch_tma_batch<__half>(chans, nchan, grid, threads, smem, odd, s);
 }
 
+
+void launch_links_lp(int precision, const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s)
+{
+    if (precision == 32) launch_links_pass<float>(tab, n, blocks, odd, s);
+    else launch_links_pass<__half>(tab, n, blocks, odd, s);
+}
+
 }  // namespace dnslbm
