@@ -85,6 +85,7 @@ struct dnslbm_ctx {
     int have_state = 0;
     int odd = 0;  // parity of the next step (1: populations are post-collision, swapped)
     long long done = 0;
+    int slab_next = 0;  // next x of a state loaded in slabs
     char err[512] = {0};
 };
 
@@ -256,6 +257,8 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     if (deck->xdv < 2 || deck->ydv < 2 || deck->zdv < 3)
         return fail(c, DNSLBM_ERR_ARG, "grid %dx%dx%d too small (need xdv,ydv >= 2, zdv >= 3)", deck->xdv, deck->ydv,
                     deck->zdv);
+    if (deck->ydv > 65535)
+        return fail(c, DNSLBM_ERR_ARG, "ydv %d above 65535 (one grid row of blocks per y in the state I/O)", deck->ydv);
     if ((long long)(deck->xdv + 8) * deck->ydv * deck->zdv >= (1LL << 31))
         return fail(c, DNSLBM_ERR_ARG, "grid of %lld cells exceeds 2^31", (long long)deck->xdv * deck->ydv * deck->zdv);
     if (!(deck->omega > 0.0 && deck->omega < 2.0)) return fail(c, DNSLBM_ERR_ARG, "omega %g outside (0,2)", deck->omega);
@@ -604,6 +607,40 @@ extern "C" int dnslbm_load_state(dnslbm_ctx *c, const double *state)
         launch_io(c->deck.precision, 1, p, x0, n, c->staging, nullptr, c->stream);
         CK(cudaGetLastError());
     }
+    c->have_state = 1;
+    return initial_reduce(c);
+}
+
+extern "C" int dnslbm_load_state_slab(dnslbm_ctx *c, int x0, int nxs, const double *slab)
+{
+    if (!c || !slab) return fail(c, DNSLBM_ERR_ARG, "null argument");
+    if (nxs < 1 || x0 < 0 || x0 + nxs > c->nx)
+        return fail(c, DNSLBM_ERR_ARG, "slab x in [%d, %d) is not inside [0, %d)", x0, x0 + nxs, c->nx);
+    if (x0 != 0 && x0 != c->slab_next)
+        return fail(c, DNSLBM_ERR_STATE, "slabs come in order of x: expected x0 = %d (or 0 to start over), got %d",
+                    c->slab_next, x0);
+    CK(cudaSetDevice(c->deck.device));
+    if (x0 == 0) {
+        int rc = reset_counters(c);
+        if (rc) return rc;
+        c->have_state = 0;
+    }
+    IoArgs p = io_args(c);
+    const size_t plane = (size_t)c->ny * (c->nz + 2) * Q;  // doubles per x
+    const int xchunk = (int)std::max<size_t>(1, c->staging_bytes / (plane * sizeof(double)));
+    for (int i = 0; i < nxs; i += xchunk) {
+        const int n = std::min(xchunk, nxs - i);
+        CK(cudaMemcpyAsync(c->staging, slab + (size_t)i * plane, (size_t)n * plane * sizeof(double),
+                           cudaMemcpyHostToDevice, c->stream));
+        launch_io(c->deck.precision, 1, p, x0 + i, n, c->staging, nullptr, c->stream);
+        CK(cudaGetLastError());
+    }
+    c->slab_next = x0 + nxs;
+    if (c->slab_next < c->nx) {
+        CK(cudaStreamSynchronize(c->stream));  // the caller may reuse its slab buffer
+        return DNSLBM_OK;
+    }
+    c->slab_next = 0;
     c->have_state = 1;
     return initial_reduce(c);
 }

@@ -90,38 +90,51 @@ __device__ __forceinline__ void gather_natural(const IoArgs &p, int x, int y, in
     }
 }
 
-// cells of x-slab [x0, x0+nxc), one thread per fluid cell; AoS index
-// ((x-x0)*ny + y)*zd + (z+1)
+// Tiles of kTX consecutive x by kTZ consecutive z of one y, through shared
+// memory: the SoA side is read or written along x (coalesced per
+// direction), the AoS side along a cell's kTZ * 19 contiguous doubles.  AoS
+// index of x-slab [x0, x0+nxc): ((x-x0)*ny + y)*zd + (z+1), times 19.
+constexpr int kTX = 32, kTZ = 8;
+
 template <typename T>
-__global__ void export_kernel(const IoArgs p, int x0, int nxc, double *aos)
+__global__ void __launch_bounds__(kTX * kTZ) export_kernel(const IoArgs p, int x0, int nxc, double *aos)
 {
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long ncell = (long long)nxc * p.ny * p.nz;
-    if (tid >= ncell) return;
-    const int z = (int)(tid % p.nz);
-    const int y = (int)((tid / p.nz) % p.ny);
-    const int xl = (int)(tid / ((long long)p.nz * p.ny));
-    double f[Q];
-    gather_natural<T>(p, x0 + xl, y, z, f);
-    double *o = aos + (((size_t)xl * p.ny + y) * (p.nz + 2) + (z + 1)) * Q;
+    __shared__ double sh[kTX][kTZ * Q + 1];
+    const int tx = threadIdx.x % kTX, tz = threadIdx.x / kTX;
+    const int xl0 = blockIdx.x * kTX, z0 = blockIdx.y * kTZ, y = blockIdx.z;
+    if (xl0 + tx < nxc && z0 + tz < p.nz) {
+        double f[Q];
+        gather_natural<T>(p, x0 + xl0 + tx, y, z0 + tz, f);
 #pragma unroll
-    for (int a = 0; a < Q; ++a) o[a] = f[a];
+        for (int a = 0; a < Q; ++a) sh[tx][tz * Q + a] = f[a];
+    }
+    __syncthreads();
+    const int per_x = min(kTZ, p.nz - z0) * Q;
+    for (int i = threadIdx.x; i < kTX * per_x; i += blockDim.x) {
+        const int xi = i / per_x, r = i - xi * per_x;
+        if (xl0 + xi < nxc) aos[(((size_t)(xl0 + xi) * p.ny + y) * (p.nz + 2) + (z0 + 1)) * Q + r] = sh[xi][r];
+    }
 }
 
 template <typename T>
-__global__ void import_kernel(const IoArgs p, int x0, int nxc, const double *aos)
+__global__ void __launch_bounds__(kTX * kTZ) import_kernel(const IoArgs p, int x0, int nxc, const double *aos)
 {
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long ncell = (long long)nxc * p.ny * p.nz;
-    if (tid >= ncell) return;
-    const int z = (int)(tid % p.nz);
-    const int y = (int)((tid / p.nz) % p.ny);
-    const int xl = (int)(tid / ((long long)p.nz * p.ny));
-    const double *i = aos + (((size_t)xl * p.ny + y) * (p.nz + 2) + (z + 1)) * Q;
-    const int c = (z * p.ny + y) * p.pitch + (x0 + xl);
-    const bool solid = p.textured == 2 && (cell_links(p.band_of, p.links, p.nx, p.ny, x0 + xl, y, z) & 1u);
+    __shared__ double sh[kTX][kTZ * Q + 1];
+    const int tx = threadIdx.x % kTX, tz = threadIdx.x / kTX;
+    const int xl0 = blockIdx.x * kTX, z0 = blockIdx.y * kTZ, y = blockIdx.z;
+    const int per_x = min(kTZ, p.nz - z0) * Q;
+    for (int i = threadIdx.x; i < kTX * per_x; i += blockDim.x) {
+        const int xi = i / per_x, r = i - xi * per_x;
+        if (xl0 + xi < nxc) sh[xi][r] = aos[(((size_t)(xl0 + xi) * p.ny + y) * (p.nz + 2) + (z0 + 1)) * Q + r];
+    }
+    __syncthreads();
+    const int x = x0 + xl0 + tx, z = z0 + tz;
+    if (xl0 + tx >= nxc || z >= p.nz) return;
+    const int c = (z * p.ny + y) * p.pitch + x;
+    const bool solid = p.textured == 2 && (cell_links(p.band_of, p.links, p.nx, p.ny, x, y, z) & 1u);
 #pragma unroll
-    for (int a = 0; a < Q; ++a) Nat<T>::st(static_cast<T *>(p.pop[a]) + c, solid ? Nat<float>::wq(a) : i[a], a);
+    for (int a = 0; a < Q; ++a)
+        Nat<T>::st(static_cast<T *>(p.pop[a]) + c, solid ? Nat<float>::wq(a) : sh[tx][tz * Q + a], a);
 }
 
 // solid cells inside the flow -> rest state (after the flags change)
@@ -263,12 +276,10 @@ template <typename T>
 static void io_dispatch(int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s)
 {
     const int bs = 256;
-    if (what == 0) {
-        const long long n = (long long)nxc * p.ny * p.nz;
-        export_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p, x0, nxc, a);
-    } else if (what == 1) {
-        const long long n = (long long)nxc * p.ny * p.nz;
-        import_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p, x0, nxc, a);
+    if (what == 0 || what == 1) {
+        const dim3 grid((nxc + kTX - 1) / kTX, (p.nz + kTZ - 1) / kTZ, p.ny);
+        if (what == 0) export_kernel<T><<<grid, kTX * kTZ, 0, s>>>(p, x0, nxc, a);
+        else import_kernel<T><<<grid, kTX * kTZ, 0, s>>>(p, x0, nxc, a);
     } else if (what == 2) {
         const long long n = (long long)p.pitch * p.ny * p.nz;
         rest_kernel<T><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(p);

@@ -63,6 +63,7 @@ def lib():
     L.dnslbm_init_rest.argtypes = [vp]
     L.dnslbm_load_state.argtypes = [vp, dp]
     L.dnslbm_store_state.argtypes = [vp, dp]
+    L.dnslbm_load_state_slab.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
     L.dnslbm_step.argtypes = [vp, ctypes.c_long]
     L.dnslbm_steps_done.argtypes = [vp]
     L.dnslbm_steps_done.restype = ctypes.c_long
@@ -159,6 +160,17 @@ class Channel:
         s = np.ascontiguousarray(state, np.float64)
         assert s.shape == self.state_shape, (s.shape, self.state_shape)
         self._ck(self.L.dnslbm_load_state(self.h, _dp(s)))
+
+    def load_state_slab(self, x0, slab):
+        """Part of a state: x in [x0, x0 + len(slab)) (dnslbm_load_state_slab)."""
+        s = np.ascontiguousarray(slab, np.float64)
+        assert s.shape[1:] == self.state_shape[1:], (s.shape, self.state_shape)
+        self._ck(self.L.dnslbm_load_state_slab(self.h, x0, s.shape[0], _dp(s)))
+
+    def load_state_slabs(self, slabs):
+        """A whole state from (x0, slab) pairs in order of x."""
+        for x0, slab in slabs:
+            self.load_state_slab(x0, slab)
 
     def store_state(self, out=None):
         if out is None:

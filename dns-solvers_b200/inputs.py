@@ -86,6 +86,69 @@ def turbulent_state(nx, ny, nz, ubulk, amp, seed, modes=4, kmax=6):
     return s
 
 
+def turbulent_slabs(nx, ny, nz, ubulk, amp, seed, slab=16, flags=None, workers=None, modes=4, kmax=6):
+    """The field of turbulent_state (same construction and seed; the rms
+    normalisation is summed slab by slab) as x-slabs (x0, state[x0:x0+n]) in
+    order, for grids whose whole state does not fit host memory comfortably.
+    Slabs are made by a thread pool (numpy releases the GIL), `workers` at a
+    time; solid cells of `flags` (-1 inside the flow) are set to rest."""
+    from concurrent.futures import ThreadPoolExecutor
+    import os
+    rng = np.random.default_rng(seed)
+    z = zeta(nz)
+    H = float(nz)
+    kx = np.fft.fftfreq(nx, 1.0 / nx)[:, None]
+    ky = np.fft.rfftfreq(ny, 1.0 / ny)[None, :]
+    mask = (np.abs(kx) <= kmax) & (np.abs(ky) <= kmax) & ((kx != 0) | (ky != 0))
+    B, Bx, By = (np.zeros((3, modes, nx, ny)) for _ in range(3))
+    for c in range(3):
+        for m in range(modes):
+            spec = (rng.standard_normal((nx, ny // 2 + 1)) + 1j * rng.standard_normal((nx, ny // 2 + 1))) * mask
+            B[c, m] = np.fft.irfft2(spec, s=(nx, ny))
+            Bx[c, m] = np.fft.irfft2(spec * (2j * np.pi * kx / nx), s=(nx, ny))
+            By[c, m] = np.fft.irfft2(spec * (2j * np.pi * ky / ny), s=(nx, ny))
+    m = np.arange(1, modes + 1)[:, None]
+    pz = np.sin(np.pi * z)[None] * np.sin(m * np.pi * z[None])
+    dpz = (np.pi / H) * (np.cos(np.pi * z)[None] * np.sin(m * np.pi * z[None])
+                         + m * np.sin(np.pi * z)[None] * np.cos(m * np.pi * z[None]))
+
+    def perturbation(x0, x1):
+        sl = slice(x0, x1)
+        up = np.empty((x1 - x0, ny, nz, 3), np.float64)
+        up[..., 0] = np.einsum("mxy,mz->xyz", By[2][:, sl], pz) - np.einsum("mxy,mz->xyz", B[1][:, sl], dpz)
+        up[..., 1] = np.einsum("mxy,mz->xyz", B[0][:, sl], dpz) - np.einsum("mxy,mz->xyz", Bx[2][:, sl], pz)
+        up[..., 2] = np.einsum("mxy,mz->xyz", Bx[1][:, sl], pz) - np.einsum("mxy,mz->xyz", By[0][:, sl], pz)
+        return up
+
+    bounds = [(x0, min(x0 + slab, nx)) for x0 in range(0, nx, slab)]
+    workers = workers or min(16, os.cpu_count() or 1)
+    with ThreadPoolExecutor(workers) as ex:
+        ss = sum(ex.map(lambda b: float((perturbation(*b) ** 2).sum()), bounds))
+        scale = amp * ubulk / max(np.sqrt(ss / (nx * ny * nz)), 1e-300)
+        lam = 1.5 * ubulk * 4 * z * (1 - z)
+        one = np.ones((ny, nz))
+
+        def make(b):
+            up = perturbation(*b)
+            up *= scale
+            up[..., 0] += lam
+            st = np.zeros((b[1] - b[0], ny, nz + 2, 19))
+            for i in range(b[1] - b[0]):
+                st[i, :, 1:nz + 1] = equilibrium(one, up[i])
+            if flags is not None:
+                st = rest_solids(st, flags[b[0]:b[1]])
+            return st
+
+        pending = []
+        for b in bounds:
+            pending.append((b[0], ex.submit(make, b)))
+            if len(pending) > workers:
+                x0, f = pending.pop(0)
+                yield x0, f.result()
+        for x0, f in pending:
+            yield x0, f.result()
+
+
 # ------------------------------------------------------------------ textures
 def flags_smooth(nx, ny, nz):
     """solid_init.c:18-45 on the periodic grid: no-slip walls, fluid inside."""
@@ -239,6 +302,9 @@ def workload(name):
         return channel_180(100, "longitudinal", gap=g, width=w)
     if name == "riblets180":  # the Re_tau 180 grid with riblets of height 8, spacing 16
         return channel(100, 180.0, "riblets", name="riblets_re180_h100", height=8, spacing=16)
+    if name.startswith("riblets180_h"):  # smaller half-heights, same riblets
+        h = int(name[len("riblets180_h"):])
+        return channel(h, 180.0, "riblets", name=f"riblets_re180_h{h}", height=8, spacing=16)
     if name == "riblets395":  # 1256 x 408 x 628 incl. walls, riblets of height 8, spacing 16
         w = channel(200, 395.0, "riblets", name="riblets_re395_h200", height=8, spacing=16)
         w.nx, w.nz = 1256, 406  # the riblets take the first planes at each wall

@@ -116,6 +116,12 @@ int dnslbm_init_rest(dnslbm_ctx *ctx);
  * read, :494-497 write).  Wall-plane entries are ignored on load and written
  * as zeros on store.  Loading resets the step counter. */
 int dnslbm_load_state(dnslbm_ctx *ctx, const double *state);
+/* The same in x-slabs, like the reference's per-rank read of its x-range of
+ * the lbf file (dns-const-q-xycut.c:405-416): `slab` holds x in [x0, x0+nxs)
+ * in the lbf layout (nxs * ydv * zd * 19 doubles).  Slabs come in order of
+ * x; x0 = 0 starts a new state (and resets the step counter), the slab that
+ * ends at xdv completes it.  Until then the context holds no state. */
+int dnslbm_load_state_slab(dnslbm_ctx *ctx, int x0, int nxs, const double *slab);
 int dnslbm_store_state(dnslbm_ctx *ctx, double *state);
 
 /* Advance nsteps time steps on the device.  Each step is the reference's loop
