@@ -22,6 +22,8 @@ void launch_reduce_lp(int precision, const StepArgs &p, dim3 grid, dim3 block, c
 void launch_io(int precision, int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s);
 void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int rows, int pass, const double *mean,
                   double *partials, double *plane_out, cudaStream_t s);
+void launch_stats_sample(int nz, double np, const double *planes, double *mean, double *acc, bool accumulate,
+                         cudaStream_t s);
 int tma_prepare_f64(size_t smem);
 int tma_occupancy_f64(int threads, size_t smem);
 void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
@@ -69,6 +71,8 @@ struct dnslbm_ctx {
     double *staging = nullptr;  // device AoS staging for I/O
     size_t staging_bytes = 0;
     double *stat_partials = nullptr, *stat_planes = nullptr, *stat_mean = nullptr;
+    double *stat_acc = nullptr;  // [9][nz] running sums of the time average
+    long stat_samples = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;                // the per-cell pass runs here beside the bulk kernel
     cudaEvent_t fj[2] = {nullptr, nullptr};     // fork / join of the side stream
@@ -158,7 +162,7 @@ static void free_all(dnslbm_ctx *c)
     void *ptrs[] = {c->popmem,     c->wallmask,   c->force,         c->shift,       c->partials,
                     c->plane_sums, c->logs,       c->step_ctr,      c->status,      c->plane_ctr,
                     c->total_ctr,  c->staging,    c->stat_partials, c->stat_planes, c->stat_mean,
-                    c->band_of,    c->links,      c->plane_list,    c->d_llaunch};
+                    c->band_of,    c->links,      c->plane_list,    c->d_llaunch,   c->stat_acc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : c->ev)
@@ -357,6 +361,7 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         {(void **)&c->stat_mean, (size_t)c->nz * 4 * sizeof(double)},
         {(void **)&c->band_of, (size_t)c->nz * sizeof(int)},
         {(void **)&c->plane_list, (size_t)c->nz * sizeof(int)},
+        {(void **)&c->stat_acc, (size_t)9 * c->nz * sizeof(double)},
         {(void **)&c->d_llaunch, sizeof(LinksLaunch)},
     };
     for (auto &a : al) {
@@ -819,6 +824,55 @@ extern "C" int dnslbm_moments(dnslbm_ctx *c, double *vel, double *den)
         if (den) CK(cudaMemcpyAsync(den + off, dd, cells * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     }
     CK(cudaStreamSynchronize(c->stream));
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_stats_accumulate(dnslbm_ctx *c)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    CK(cudaSetDevice(c->deck.device));
+    const double np = (double)c->nx * c->ny;
+    IoArgs p = io_args(c);
+    launch_stats(c->deck.precision, p, c->grid, c->block, c->rows, 0, nullptr, c->stat_partials, c->stat_planes,
+                 c->stream);
+    launch_stats_sample(c->nz, np, c->stat_planes, c->stat_mean, nullptr, false, c->stream);
+    launch_stats(c->deck.precision, p, c->grid, c->block, c->rows, 1, c->stat_mean, c->stat_partials, c->stat_planes,
+                 c->stream);
+    launch_stats_sample(c->nz, np, c->stat_planes, c->stat_mean, c->stat_acc, true, c->stream);
+    CK(cudaGetLastError());
+    ++c->stat_samples;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_stats_average(dnslbm_ctx *c, double *out, long *nsamples)
+{
+    if (!c || !out) return fail(c, DNSLBM_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->deck.device));
+    const int nz = c->nz, zd = nz + 2;
+    std::vector<double> acc((size_t)9 * nz);
+    CK(cudaMemcpyAsync(acc.data(), c->stat_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memset(out, 0, sizeof(double) * 9 * zd);
+    if (nsamples) *nsamples = c->stat_samples;
+    if (c->stat_samples == 0) return DNSLBM_OK;
+    const double n = (double)c->stat_samples;
+    for (int r = 0; r < 9; ++r) {
+        const bool rms = r == 3 || r == 4 || r == 5 || r == 8;
+        for (int z = 0; z < nz; ++z) {
+            const double v = acc[(size_t)r * nz + z] / n;
+            out[(size_t)r * zd + z + 1] = rms ? std::sqrt(v) : v;
+        }
+    }
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_stats_reset(dnslbm_ctx *c)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    CK(cudaSetDevice(c->deck.device));
+    CK(cudaMemsetAsync(c->stat_acc, 0, (size_t)9 * c->nz * sizeof(double), c->stream));
+    c->stat_samples = 0;
     return DNSLBM_OK;
 }
 

@@ -271,6 +271,36 @@ __global__ void plane_reduce_kernel(const double *partials, int bpp, double *out
         for (int i = 0; i < NS; ++i) out[z * NS + i] = s[i];
 }
 
+// On-device time averages of the plane statistics: the plane means of a
+// sample from its pass-0 sums, and the running FP64 sums of the sample's
+// nine statistics rows (statistics.c order: u, v, w means, u', v', w' rms,
+// <u'w'>, rho mean, rho' rms) with each rms entered as its square, which is
+// how the reference's post-processing pools rms values over a time window
+// (TKE-budget/postprocessing/time_stats.c:203-213).
+__global__ void stats_means_kernel(const double *planes, int nz, double np, double *mean)
+{
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nz) return;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mean[z * 4 + i] = planes[z * NS + i] / np;
+}
+
+__global__ void stats_accumulate_kernel(const double *planes, const double *mean, int nz, double np, double *acc)
+{
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nz) return;
+    const double *pl = planes + (size_t)z * NS;
+    acc[0 * nz + z] += mean[z * 4 + 0];
+    acc[1 * nz + z] += mean[z * 4 + 1];
+    acc[2 * nz + z] += mean[z * 4 + 2];
+    acc[3 * nz + z] += pl[0] / np;
+    acc[4 * nz + z] += pl[1] / np;
+    acc[5 * nz + z] += pl[2] / np;
+    acc[6 * nz + z] += pl[3] / np;
+    acc[7 * nz + z] += mean[z * 4 + 3];
+    acc[8 * nz + z] += pl[4] / np;
+}
+
 // ---------------------------------------------------------------- launchers
 template <typename T>
 static void io_dispatch(int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s)
@@ -297,6 +327,14 @@ void launch_io(int precision, int what, const IoArgs &p, int x0, int nxc, double
     if (precision == 64) io_dispatch<double>(what, p, x0, nxc, a, b, s);
     else if (precision == 32) io_dispatch<float>(what, p, x0, nxc, a, b, s);
     else io_dispatch<__half>(what, p, x0, nxc, a, b, s);
+}
+
+void launch_stats_sample(int nz, double np, const double *planes, double *mean, double *acc, bool accumulate,
+                         cudaStream_t s)
+{
+    const int bs = 128, nb = (nz + bs - 1) / bs;
+    if (accumulate) stats_accumulate_kernel<<<nb, bs, 0, s>>>(planes, mean, nz, np, acc);
+    else stats_means_kernel<<<nb, bs, 0, s>>>(planes, nz, np, mean);
 }
 
 void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int rows, int pass, const double *mean,

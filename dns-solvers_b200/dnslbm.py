@@ -70,6 +70,9 @@ def lib():
     L.dnslbm_logs.argtypes = [vp, ctypes.c_long, ctypes.c_long, dp]
     L.dnslbm_get_force.argtypes = [vp, dp]
     L.dnslbm_statistics.argtypes = [vp, dp]
+    L.dnslbm_stats_accumulate.argtypes = [vp]
+    L.dnslbm_stats_average.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_long)]
+    L.dnslbm_stats_reset.argtypes = [vp]
     L.dnslbm_moments.argtypes = [vp, dp, dp]
     L.dnslbm_step_timed.argtypes = [vp, ctypes.c_long, dp, dp, dp]
     L.dnslbm_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
@@ -208,6 +211,19 @@ class Channel:
         self._ck(self.L.dnslbm_statistics(self.h, _dp(out)))
         return out.reshape(9, zd)
 
+    def stats_accumulate(self):
+        """Add a sample of the current plane statistics to the device average."""
+        self._ck(self.L.dnslbm_stats_accumulate(self.h))
+
+    def stats_average(self):
+        """(averages [9, zd], number of samples) of the device time average."""
+        out = np.zeros((9, self.shape[2] + 2), np.float64)
+        n = ctypes.c_long()
+        self._ck(self.L.dnslbm_stats_average(self.h, _dp(out), ctypes.byref(n)))
+        return out, n.value
+
+    def stats_reset(self):
+        self._ck(self.L.dnslbm_stats_reset(self.h))
     def moments(self):
         x, y, z = self.shape
         vel = np.zeros((x, y, z + 2, 3))

@@ -15,7 +15,9 @@
  * compile-time names Rebs ub zdv ydv xdv TSTR TEND CFL ITER (definitions.h:
  * 30-52) and RSLIP / PSLIP (set to 1 to select those textures with the
  * reference's constants), plus
- *   TEXTURE smooth|ridges|transverse|posts   GAP WIDTH   PGX PWX PGY PWY
+ *   TEXTURE smooth|ridges|transverse|posts|riblets   GAP WIDTH   PGX PWX PGY PWY
+ *   RIBH RIBS (riblet height and spacing; riblets select the general wall
+ *   rule, DNSLBM_BC_GENERAL)
  *   PRECISION 64|32|16   FORCE q|g   GX   DEVICE   OMEGA (overrides Rebs)
  *
  * Files written (formats of the reference):
@@ -40,7 +42,7 @@
 typedef struct {
     double Rebs, ub, CFL, GX, OMEGA;
     int zdv, ydv, xdv, TSTR, TEND, ITER, RSLIP, PSLIP;
-    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY;
+    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS;
     char TEXTURE[32], FORCE[8];
 } Deck;
 
@@ -64,6 +66,8 @@ static void deck_defaults(Deck *d)
     d->PWX = 2;
     d->PGY = 2;
     d->PWY = 2;
+    d->RIBH = 8;
+    d->RIBS = 16;
     strcpy(d->TEXTURE, "smooth");
     strcpy(d->FORCE, "q");
 }
@@ -75,7 +79,7 @@ static int deck_set(Deck *d, const char *k, const char *v)
 #define STR(N) if (!strcmp(k, #N)) { snprintf(d->N, sizeof d->N, "%s", v); return 0; }
     DBL(Rebs) DBL(ub) DBL(CFL) DBL(GX) DBL(OMEGA)
     INT(zdv) INT(ydv) INT(xdv) INT(TSTR) INT(TEND) INT(ITER) INT(RSLIP) INT(PSLIP)
-    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY)
+    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS)
     STR(TEXTURE) STR(FORCE)
 #undef DBL
 #undef INT
@@ -172,7 +176,8 @@ int main(int argc, char **argv)
 
     dnslbm_deck dk = {D.xdv, D.ydv, D.zdv, omega, D.ub, D.GX,
                       D.FORCE[0] == 'g' ? DNSLBM_FORCE_CONST_G : DNSLBM_FORCE_CONST_Q,
-                      D.PRECISION, DNSLBM_BC_REFERENCE, 0, D.DEVICE};
+                      D.PRECISION, strcmp(D.TEXTURE, "riblets") ? DNSLBM_BC_REFERENCE : DNSLBM_BC_GENERAL, 0,
+                      D.DEVICE};
     dnslbm_ctx *c = NULL;
     int rc = dnslbm_create(&dk, &c);
     if (rc) return die(NULL, rc, "dnslbm_create");
@@ -189,6 +194,8 @@ int main(int argc, char **argv)
     else if (!strcmp(D.TEXTURE, "ridges")) tex_longitudinal(D.xdv, D.ydv, D.zdv, D.GAP, D.WIDTH, flags);
     else if (!strcmp(D.TEXTURE, "transverse")) tex_transverse(D.xdv, D.ydv, D.zdv, D.GAP, D.WIDTH, flags);
     else if (!strcmp(D.TEXTURE, "posts")) tex_posts(D.xdv, D.ydv, D.zdv, D.PGX, D.PWX, D.PGY, D.PWY, flags);
+    else if (!strcmp(D.TEXTURE, "riblets") && D.RIBH > 0 && D.RIBS > 1)
+        tex_riblets(D.xdv, D.ydv, D.zdv, D.RIBH, D.RIBS, flags);
     else {
         fprintf(stderr, "run-dns: unknown texture %s\n", D.TEXTURE);
         return 2;

@@ -5,6 +5,7 @@
  */
 #include "textures.h"
 
+#include <math.h>
 #include <string.h>
 
 #define IDX(x, y, z) (((size_t)(x) * ny + (y)) * zd + (z))
@@ -57,4 +58,26 @@ void tex_posts(int nx, int ny, int nz, int gx, int wx, int gy, int wy, int8_t *f
         for (int a = 0; a < gy && j + a < ny; a++)
             for (int i = 1; i < nx; i += gx + wx)
                 for (int b = 0; b < gx && i + b < nx; b++) slip_both(nx, ny, nz, flags, i + b, j + a);
+}
+
+/* Triangular streamwise riblets cut into both no-slip walls (solid cells -1
+ * inside the flow; the general boundary mode): in each spanwise period of
+ * `spacing` cells a triangle of the given height, h(y) = height (1 -
+ * |2 y_c / spacing - 1|) with y_c = (y mod spacing) + 1/2; a cell of wall
+ * distance k - 1/2 (k = 1 the first fluid plane) is solid when below it. */
+void tex_riblets(int nx, int ny, int nz, int height, int spacing, int8_t *flags)
+{
+    const int zd = nz + 2;
+    tex_smooth(nx, ny, nz, flags);
+    for (int y = 0; y < ny; y++) {
+        const double yc = (y % spacing) + 0.5;
+        const double h = height * (1.0 - fabs(2.0 * yc / spacing - 1.0));
+        int nk = (int)ceil(h + 0.5) - 1;
+        if (nk > nz / 2) nk = nz / 2;
+        for (int k = 1; k <= nk; k++)
+            for (int x = 0; x < nx; x++) {
+                flags[IDX(x, y, k)] = -1;
+                flags[IDX(x, y, zd - 1 - k)] = -1;
+            }
+    }
 }

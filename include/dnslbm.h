@@ -140,6 +140,17 @@ int dnslbm_get_force(dnslbm_ctx *ctx, double *force);
 
 /* statistics.c:3-183 of the current state: out[9*zd]. */
 int dnslbm_statistics(dnslbm_ctx *ctx, double *out);
+/* Time averages of the plane statistics kept on the device: each
+ * dnslbm_stats_accumulate adds a sample of the current state (the rows of
+ * dnslbm_statistics) to FP64 running sums without a copy to the host;
+ * dnslbm_stats_average returns the averages in the turb-fld layout
+ * (9 * zd doubles, wall entries 0): means averaged, rms values pooled as
+ * the root of the mean square, as the reference's post-processing averages
+ * turb-fld files over a window (TKE-budget/postprocessing/time_stats.c).
+ * dnslbm_stats_reset starts a new window (dnslbm_create starts one). */
+int dnslbm_stats_accumulate(dnslbm_ctx *ctx);
+int dnslbm_stats_average(dnslbm_ctx *ctx, double *out, long *nsamples);
+int dnslbm_stats_reset(dnslbm_ctx *ctx);
 /* vel_print.c:65-99 of the current state (either pointer may be NULL). */
 int dnslbm_moments(dnslbm_ctx *ctx, double *vel, double *den);
 

@@ -36,14 +36,14 @@ def write_deck(d, tstr, extra=""):
                 f"TSTR {tstr}\nTEND {tstr + 5}\nITER {ITER}\n{extra}")
 
 
-def oracle_run(oracle_mod, s0, flags):
+def oracle_run(oracle_mod, s0, flags, bc_mode=0):
     """Logs of steps 0..ITER and the states at the output steps."""
     st = s0.copy()
     logs, snaps = [], {}
     for ss in range(ITER + 1):
         if ss % UTIME == 0:
             snaps[ss] = st.copy()
-        logs.append(oracle_mod.run(st, flags, OMEGA, ubulk=UB, const_g=False, nsteps=1)[0])
+        logs.append(oracle_mod.run(st, flags, OMEGA, ubulk=UB, const_g=False, nsteps=1, bc_mode=bc_mode)[0])
     return np.array(logs), snaps
 
 
@@ -77,6 +77,19 @@ def test_fresh_start_matches_oracle(oracle_mod, tmp_path):
     s0 = np.zeros((NX, NY, NZ + 2, 19))
     s0[:, :, 1:NZ + 1] = inputs.W
     logs, snaps = oracle_run(oracle_mod, s0, inputs.flags_smooth(NX, NY, NZ))
+    check_outputs(d, oracle_mod, logs, snaps, 0)
+
+
+def test_fresh_start_with_riblets(oracle_mod, tmp_path):
+    """TEXTURE riblets (RIBH, RIBS): solids inside the flow, general wall rule."""
+    d = str(tmp_path)
+    write_deck(d, 0, "TEXTURE riblets\nRIBH 2\nRIBS 4\n")
+    subprocess.run([RUN_DNS, "-s", "deck.txt"], cwd=d, check=True, timeout=120, capture_output=True)
+    s0 = np.zeros((NX, NY, NZ + 2, 19))
+    s0[:, :, 1:NZ + 1] = inputs.W
+    flags = inputs.flags_riblets(NX, NY, NZ, 2, 4)
+    assert (flags[:, :, 1:-1] == -1).any()
+    logs, snaps = oracle_run(oracle_mod, s0, flags, bc_mode=1)
     check_outputs(d, oracle_mod, logs, snaps, 0)
 
 
