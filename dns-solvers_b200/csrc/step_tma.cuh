@@ -175,22 +175,37 @@ __device__ __forceinline__ void copy_group(const StepArgs &p, const TmaArgs &t, 
 }
 
 // ------------------------------------------------------------------ cells
-// One cell row from the stage buffer: direction A's element x at
-// sb[A * dstride + x].
+// The k cell rows of a row group from the stage buffer: direction A's
+// element x of row j at sb[A * dstride + j * pitch + x].  The group's k * nx
+// cells are spread over the nc consumer threads as one range, so rows
+// shorter than the consumer set keep every thread busy.
 // WALL: 0 interior plane, -1 bottom plane, +1 top plane.
 template <typename T, bool ODD, bool CONSTQ, bool TEXTURED, int WALL>
-__device__ __forceinline__ void tma_row(const StepArgs &p, T *sb, int dstride, int y, int z, double G,
-                                        const double *shift, double (&acc)[NP], int nc)
+__device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride, int y0, int k, int z, double G,
+                                          const double *shift, double (&acc)[NP], int nc)
 {
     using V = RegT<T>;
     const double c0 = shift[0], c1 = shift[1], c2 = shift[2];
     const int nx = p.nx, pitch = p.pitch;
-    // low precision: this row's few cells per thread are summed in FP32,
-    // then added to the FP64 accumulators once per row
+    // low precision: a row's few cells per thread are summed in FP32, then
+    // added to the FP64 accumulators when the thread moves to another row
     float racc[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) racc[i] = 0.f;
-    for (int x = threadIdx.x; x < nx; x += nc) {
+    int j = 0, x = threadIdx.x, jr = 0;
+    while (x >= nx && j < k) x -= nx, ++j;
+    for (; j < k; x += nc) {
+        while (x >= nx) x -= nx, ++j;
+        if (j >= k) break;
+        if constexpr (!std::is_same<T, double>::value) {
+            if (j != jr) {
+#pragma unroll
+                for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i], racc[i] = 0.f;
+                jr = j;
+            }
+        }
+        const int y = y0 + j;
+        T *sbj = sb + (size_t)j * pitch;
         const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
         unsigned bits = 0x1fu;
         if (TEXTURED && WALL != 0) bits = p.wallmask[(size_t)(WALL > 0) * nx * p.ny + (size_t)y * nx + x];
@@ -213,7 +228,7 @@ __device__ __forceinline__ void tma_row(const StepArgs &p, T *sb, int dstride, i
                 v = ld_raw<T>(static_cast<const T *>(p.pop[slot]) + idx);
             } else {
                 const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
-                v = ld_raw<T>(sb + A * dstride + xs);
+                v = ld_raw<T>(sbj + A * dstride + xs);
             }
             f[ODD ? lat_opp(A) : A] = v;
         }
@@ -288,7 +303,7 @@ __device__ __forceinline__ void tma_row(const StepArgs &p, T *sb, int dstride, i
                 st_raw<T>(static_cast<T *>(p.pop[slot]) + idx, v);
             } else {
                 const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
-                st_raw<T>(sb + A * dstride + xs, v);
+                st_raw<T>(sbj + A * dstride + xs, v);
             }
         }
     }
@@ -395,12 +410,9 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
         T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
         const double *sh = shift_now + z * 3;
         constexpr bool TXT = TEX != 0;
-        for (int j = 0; j < k; ++j) {
-            T *sbj = sb + (size_t)j * p.pitch;
-            if (z == 0) tma_row<T, ODD, CONSTQ, TXT, -1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
-            else if (z == p.nz - 1) tma_row<T, ODD, CONSTQ, TXT, 1>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
-            else tma_row<T, ODD, CONSTQ, TXT, 0>(p, sbj, dstride, y0 + j, z, G, sh, acc, nc);
-        }
+        if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        else if (z == p.nz - 1) tma_group<T, ODD, CONSTQ, TXT, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        else tma_group<T, ODD, CONSTQ, TXT, 0>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
         fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);

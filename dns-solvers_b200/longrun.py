@@ -109,7 +109,8 @@ def main():
     ap.add_argument("--spinup", type=int, default=0, help="steps before the averaging window")
     ap.add_argument("--steps", type=int, default=50000, help="steps in the averaging window")
     ap.add_argument("--sample", type=int, default=100)
-    ap.add_argument("--precisions", default="64,64p,32,16", help="64p: FP64 control from a perturbed field")
+    ap.add_argument("--precisions", default="64,64p,32,16",
+                    help="64p: FP64 control from a perturbed field (64pA: perturbation amplitude A)")
     ap.add_argument("--control-amp", type=float, default=1e-7, help="relative perturbation of the 64p control")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
@@ -122,13 +123,14 @@ def main():
     runs = []
     for p in a.precisions.split(","):
         init = s0
-        if p == "64p":
+        if p.startswith("64p"):
+            amp = float(p[3:]) if len(p) > 3 else a.control_amp
             rng = np.random.default_rng(a.seed + 1)
-            init = s0 * (1.0 + a.control_amp * rng.standard_normal(s0.shape))
+            init = s0 * (1.0 + amp * rng.standard_normal(s0.shape))
             if inputs.needs_general(wl):
                 init = inputs.rest_solids(init, flags)
         try:
-            r = run_one(wl, init, flags, int(p.rstrip("p")), a.spinup, a.steps, a.sample)
+            r = run_one(wl, init, flags, int(p[:2]), a.spinup, a.steps, a.sample)
         except dnslbm.DnsLbmError as e:  # e.g. a NaN wall stress: reported, not fatal
             r = {"failed": str(e)}
         r["run"] = p
