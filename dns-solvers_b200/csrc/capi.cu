@@ -34,13 +34,12 @@ void launch_tma_lp(int precision, const StepArgs &p, const TmaArgs &t, int grid,
                    int tex, cudaStream_t s);
 int tma_batch_prepare_f64(size_t smem);
 int tma_batch_occupancy_f64(int threads, size_t smem);
-void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, const int *items, const int2 *contrib, int grid,
-                          int threads, size_t smem, int stages, int stage_bytes, bool odd, cudaStream_t s);
+void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem, bool odd,
+                          cudaStream_t s);
 int tma_batch_prepare_lp(int precision, size_t smem);
 int tma_batch_occupancy_lp(int precision, int threads, size_t smem);
-void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, const int *items,
-                         const int2 *contrib, int grid, int threads, size_t smem, int stages, int stage_bytes, bool odd,
-                         cudaStream_t s);
+void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem,
+                         bool odd, cudaStream_t s);
 void launch_links_f64(const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s);
 void launch_links_lp(int precision, const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s);
 }  // namespace dnslbm
@@ -182,6 +181,10 @@ extern "C" const char *dnslbm_last_error(const dnslbm_ctx *c) { return c ? c->er
 // groups in flight and `consumers` compute threads (+ one producer warp);
 // bps > 0 caps the blocks per SM.  Returns 0 when the configuration runs on
 // this device (and selects it), -1 otherwise (the previous choice stays).
+// Dynamic shared memory the step kernels may be given: the device's opt-in
+// maximum less this reserve for their static shared memory (about 2.5 KB).
+constexpr size_t kStaticSmemReserve = 4096;
+
 // Row groups of the row-pipelined kernel over its planes (all planes, or the
 // planes without link masks) shared among tma_target blocks.
 static void tma_layout(dnslbm_ctx *c)
@@ -205,12 +208,12 @@ static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bp
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->deck.device);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->deck.device);
     const size_t smem = (size_t)stages * smem_stage + 16 * (size_t)stages;  // + full/empty mbarriers
-    if (stages < 2 || smem > (size_t)maxsmem || nsm <= 0) return -1;
+    const size_t cap = (size_t)maxsmem - kStaticSmemReserve;  // room for the kernels' static shared memory
+    if (stages < 2 || smem > cap || nsm <= 0) return -1;
     const int threads = consumers + 32;
     // the kernels may use up to the device's opt-in shared memory (a batch can
     // give a channel a larger stage than its own shape)
-    const int prep = c->deck.precision == 64 ? tma_prepare_f64((size_t)maxsmem)
-                                             : tma_prepare_lp(c->deck.precision, (size_t)maxsmem);
+    const int prep = c->deck.precision == 64 ? tma_prepare_f64(cap) : tma_prepare_lp(c->deck.precision, cap);
     int occ = prep ? 0
                    : (c->deck.precision == 64 ? tma_occupancy_f64(threads, smem)
                                               : tma_occupancy_lp(c->deck.precision, threads, smem));
@@ -1045,12 +1048,6 @@ struct dnslbm_batch {
     cudaStream_t stream = nullptr;
     ChannelLaunch *d_launch = nullptr;
     LinksLaunch *d_links = nullptr;  // channels with planes next to solids
-    int *d_items = nullptr;          // [grid + 1] first row group of each block in the list of all channels
-    int2 *d_contrib = nullptr;       // per channel and plane: first contributing block, number of them
-    std::vector<int> items;          // host copies of the two tables
-    std::vector<int2> contrib;
-    std::vector<int> first_item, contrib_off;
-    int stage_bytes = 0;
     int nlinks = 0, links_blocks = 0;
     int target = 0;                  // resident blocks of the row-pipelined kernel
     int grid = 0, threads = 0;
@@ -1102,8 +1099,6 @@ extern "C" void dnslbm_batch_destroy(dnslbm_batch *b)
         if (e) cudaEventDestroy(e);
     if (b->d_launch) cudaFree(b->d_launch);
     if (b->d_links) cudaFree(b->d_links);
-    if (b->d_items) cudaFree(b->d_items);
-    if (b->d_contrib) cudaFree(b->d_contrib);
     for (auto &e : b->fj)
         if (e) cudaEventDestroy(e);
     if (b->side) cudaStreamDestroy(b->side);
@@ -1116,70 +1111,49 @@ extern "C" void dnslbm_batch_destroy(dnslbm_batch *b)
 // (228 KB per SM, 1 KB of it reserved per block, the static shared memory of
 // the kernel on top).
 constexpr size_t kBatchBudget1 = 220 * 1024, kBatchBudget2 = 108 * 1024, kBatchBudget3 = 70 * 1024;
-constexpr int kMaxBatchBlocks = 4096;  // resident blocks of the batched kernel, an upper bound
 
-// The row groups of every channel's planes without link masks, in one list,
-// cut into one contiguous range per resident block so that every block moves
-// about the same number of cells (a range may run from one channel into the
-// next); per channel and plane the first block that works on it and how
-// many do; and the block count of the per-cell pass over the planes with
-// link masks.  A change of either grid invalidates the captured graphs.
+// Row groups of every channel's planes without link masks shared among the
+// resident blocks, each block taking whole row groups of one channel and
+// about the same number of cells, and the block count of the per-cell pass
+// over the planes with link masks.  A change of
+// either grid invalidates the captured graphs.
 static void batch_layout(dnslbm_batch *b)
 {
-    const int n = (int)b->ch.size();
-    b->first_item.assign(n, 0);
-    b->contrib_off.assign(n, 0);
-    std::vector<double> cum;  // cells up to and including each item
+    // a common amount of work per block (cells of whole row groups), the
+    // smallest for which the blocks fit the resident set at once
     double total = 0;
-    int lblocks = 0, nl = 0, ncontrib = 0;
-    for (int i = 0; i < n; ++i) {
-        dnslbm_ctx *c = b->ch[i];
+    for (auto *c : b->ch) total += (double)c->nx * c->ny * c->nclean;
+    const int target = std::max(1, b->target);
+    auto blocks_for = [&](double w, dnslbm_ctx *c) {
+        const double cells = (double)c->nx * c->ny * c->nclean;
+        if (cells <= 0) return 0;
+        const int ng = c->tma.gpp * c->nclean;
+        const int want = std::max(1, std::min(ng, (int)std::ceil(cells / w)));
+        const int gpb = (ng + want - 1) / want;
+        return (ng + gpb - 1) / gpb;
+    };
+    double w = std::max(1.0, total / target);
+    for (int it = 0; it < 400; ++it, w *= 1.01) {
+        int sum = 0;
+        for (auto *c : b->ch) sum += blocks_for(w, c);
+        if (sum <= target) break;
+    }
+    int grid = 0, lblocks = 0, nl = 0;
+    for (auto *c : b->ch) {
         TmaArgs &t = c->tma;
-        tma_layout(c);  // keeps the channel's own single-launch shape valid
-        b->first_item[i] = (int)cum.size();
-        b->contrib_off[i] = ncontrib;
-        ncontrib += c->nclean;
-        for (int g = 0; g < t.ngroups; ++g) {
-            const int y0 = (g % t.gpp) * t.k;
-            total += (double)c->nx * std::min(t.k, c->ny - y0);
-            cum.push_back(total);
-        }
+        t.ngroups = t.gpp * c->nclean;
+        t.planes = c->nclean < c->nz ? c->plane_list : nullptr;
+        const int nb = blocks_for(w, c);
+        t.groups_per_block = nb > 0 ? (t.ngroups + nb - 1) / nb : 1;
+        c->tma_grid = nb;
+        grid += c->tma_grid;
         if (c->ndirty > 0) {
             lblocks += c->ndirty * (int)(c->grid.x * c->grid.y);
             ++nl;
         }
     }
-    const int nitems = (int)cum.size();
-    const int grid = std::min(std::max(1, b->target), nitems);
-    b->items.assign(grid + 1, 0);
-    for (int k = 1; k < grid; ++k) {
-        // first item whose cells end beyond k / grid of the total, at least one item per block
-        const double cut = total * k / grid;
-        int it = (int)(std::upper_bound(cum.begin(), cum.end(), cut) - cum.begin());
-        it = std::max(it, b->items[k - 1] + 1);
-        it = std::min(it, nitems - (grid - k));
-        b->items[k] = it;
-    }
-    b->items[grid] = nitems;
-    // contributors per plane: blocks whose range meets the plane's groups
-    b->contrib.assign(ncontrib, int2{0, 0});
-    auto block_of = [&](int item) {
-        return (int)(std::upper_bound(b->items.begin(), b->items.end(), item) - b->items.begin()) - 1;
-    };
-    for (int i = 0; i < n; ++i) {
-        const dnslbm_ctx *c = b->ch[i];
-        for (int pi = 0; pi < c->nclean; ++pi) {
-            const int a = b->first_item[i] + pi * c->tma.gpp, e = a + c->tma.gpp - 1;
-            const int b0 = block_of(a), b1 = block_of(e);
-            b->contrib[b->contrib_off[i] + pi] = int2{b0, b1 - b0 + 1};
-        }
-    }
-    if (nitems == 0) {
-        b->items.assign(1, 0);
-    }
-    const int g = nitems == 0 ? 0 : grid;
-    if (g != b->grid || lblocks != b->links_blocks) destroy_graphs(b);
-    b->grid = g;
+    if (grid != b->grid || lblocks != b->links_blocks) destroy_graphs(b);
+    b->grid = grid;
     b->links_blocks = lblocks;
     b->nlinks = nl;
 }
@@ -1206,9 +1180,9 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
     const int threads = consumers + 32;
     int maxsmem = 0;
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
-    if (smem > (size_t)maxsmem) return -1;
-    const int prep = b->precision == 64 ? tma_batch_prepare_f64((size_t)maxsmem)
-                                        : tma_batch_prepare_lp(b->precision, (size_t)maxsmem);
+    const size_t cap = (size_t)maxsmem - kStaticSmemReserve;
+    if (smem > cap) return -1;
+    const int prep = b->precision == 64 ? tma_batch_prepare_f64(cap) : tma_batch_prepare_lp(b->precision, cap);
     const int occ = prep ? 0
                          : (b->precision == 64 ? tma_batch_occupancy_f64(threads, smem)
                                                : tma_batch_occupancy_lp(b->precision, threads, smem));
@@ -1224,10 +1198,9 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
         c->tma_smem = smem;
         c->tma_target = occ * nsm;
     }
-    b->target = std::min(occ * nsm, kMaxBatchBlocks);
+    b->target = occ * nsm;
     b->threads = threads;
     b->smem = smem;
-    b->stage_bytes = (int)((smem - 16 * (size_t)stages) / stages);
     b->budget = budget;
     b->stages = stages;
     destroy_graphs(b);
@@ -1276,14 +1249,10 @@ extern "C" int dnslbm_batch_create(const dnslbm_deck *decks, int n, dnslbm_batch
     for (auto *c : b->ch) consumers = std::max(consumers, c->tma_threads - 32);
     if (batch_configure(b, kBatchBudget2, 2, consumers) && batch_configure(b, kBatchBudget1, 2, consumers))
         return bail(bfail(b, DNSLBM_ERR_ARG, "batched kernel does not fit the device"));
-    size_t contrib_cap = 0;
-    for (auto *c : b->ch) contrib_cap += (size_t)c->nz;
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess ||
         cudaMalloc(&b->d_launch, sizeof(ChannelLaunch) * n) != cudaSuccess ||
         cudaMalloc(&b->d_links, sizeof(LinksLaunch) * n) != cudaSuccess ||
-        cudaMalloc(&b->d_items, sizeof(int) * (kMaxBatchBlocks + 1)) != cudaSuccess ||
-        cudaMalloc(&b->d_contrib, sizeof(int2) * contrib_cap) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->fj[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->fj[1], cudaEventDisableTiming) != cudaSuccess)
@@ -1309,11 +1278,10 @@ static int batch_launch(dnslbm_batch *b, bool odd)
     }
     if (b->grid > 0) {
         if (b->precision == 64)
-            launch_tma_batch_f64(b->d_launch, (int)b->ch.size(), b->d_items, b->d_contrib, b->grid, b->threads, b->smem,
-                                 b->stages, b->stage_bytes, odd, b->stream);
+            launch_tma_batch_f64(b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd, b->stream);
         else
-            launch_tma_batch_lp(b->precision, b->d_launch, (int)b->ch.size(), b->d_items, b->d_contrib, b->grid,
-                                b->threads, b->smem, b->stages, b->stage_bytes, odd, b->stream);
+            launch_tma_batch_lp(b->precision, b->d_launch, (int)b->ch.size(), b->grid, b->threads, b->smem, odd,
+                                b->stream);
     }
     if (b->links_blocks > 0) {
         if (b->precision == 64) launch_links_f64(b->d_links, b->nlinks, b->links_blocks, odd, ls);
@@ -1343,14 +1311,14 @@ static int batch_run(dnslbm_batch *b, long nsteps, double *ms)
     batch_layout(b);
     std::vector<ChannelLaunch> h(n);
     std::vector<LinksLaunch> hl;
-    int lfirst = 0;
+    int first = 0, lfirst = 0;
     for (int i = 0; i < n; ++i) {
         dnslbm_ctx *c = b->ch[i];
         h[i].p = step_args(c);
         h[i].t = c->tma;
-        h[i].first_item = b->first_item[i];
+        h[i].first_block = first;
         h[i].textured = c->walls_textured;
-        h[i].contrib = b->contrib_off[i];
+        first += c->tma_grid;
         if (c->ndirty > 0) {
             LinksLaunch L{};
             L.p = h[i].p;
@@ -1365,11 +1333,6 @@ static int batch_run(dnslbm_batch *b, long nsteps, double *ms)
         }
     }
     BCK(cudaMemcpyAsync(b->d_launch, h.data(), sizeof(ChannelLaunch) * n, cudaMemcpyHostToDevice, b->stream));
-    BCK(cudaMemcpyAsync(b->d_items, b->items.data(), sizeof(int) * b->items.size(), cudaMemcpyHostToDevice,
-                        b->stream));
-    if (!b->contrib.empty())
-        BCK(cudaMemcpyAsync(b->d_contrib, b->contrib.data(), sizeof(int2) * b->contrib.size(),
-                            cudaMemcpyHostToDevice, b->stream));
     if (!hl.empty())
         BCK(cudaMemcpyAsync(b->d_links, hl.data(), sizeof(LinksLaunch) * hl.size(), cudaMemcpyHostToDevice,
                             b->stream));

@@ -434,155 +434,43 @@ __global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepA
     tma_step_body<T, ODD, CONSTQ, TEX>(p, t, blockIdx.x, tma_smem);
 }
 
-// Many independent channels in one launch.  The row groups of all channels
-// form one list (channel by channel, first_item the channel's first); block
-// b takes the contiguous range items[b] .. items[b+1]-1, the ranges cut so
-// that every block moves about the same number of cells, so one range can
-// end one channel and start the next.  A block's contribution to a plane is
-// its sub-range of that plane's groups; the host lists, per plane, the
-// first block that contributes and how many do (`contrib`), which keeps the
-// plane sums in a fixed order.
+// Many independent channels in one launch: block b belongs to the channel c
+// with first[c] <= b < first[c+1]; the channel's arguments are copied to
+// shared memory and the block runs that channel's step.
 struct ChannelLaunch {
     StepArgs p;
     TmaArgs t;
-    int first_item;  // index of the channel's first row group in the list
-    int textured;    // TEX of the channel (0 smooth, else textured walls)
-    int contrib;     // offset of the channel's per-plane (first block, count) pairs
+    int first_block;
+    int textured;  // TEX of the channel (0 smooth, else textured walls)
 };
 
-__device__ __forceinline__ int item_channel(const ChannelLaunch *chans, int nchan, int item)
-{
-    int lo = 0, hi = nchan - 1;  // the last channel whose first item is <= item
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (chans[mid].first_item <= item) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-template <bool ODD>
-__device__ __forceinline__ GroupRows group_rows_tex(const StepArgs &p, int A, int y0, int z, int wall, int tex)
-{
-    return tex ? group_rows<ODD, 1>(p, A, y0, z, wall) : group_rows<ODD, 0>(p, A, y0, z, wall);
-}
-
 template <typename T, bool ODD>
-__device__ __forceinline__ void batch_producer(const ChannelLaunch *chans, int nchan, int i0, int n, int lane,
-                                               unsigned char *smem, size_t stage_bytes, int S, uint64_t *full,
-                                               uint64_t *empty, volatile int *abort, long long *status)
-{
-    for (int i = 0; i < n + S; ++i) {
-        const int st = i % S;
-        unsigned char *stage = smem + (size_t)st * stage_bytes;
-        if (i >= S) {  // store item i - S once the consumers have released its stage
-            if (!*abort && !mbar_wait_bounded(empty + st, (uint32_t)((i / S - 1) & 1))) {
-                *abort = 1;
-                atomicExch(reinterpret_cast<unsigned long long *>(status + 1), 1ull);
-            }
-            const int item = i0 + i - S;
-            const ChannelLaunch &L = chans[item_channel(chans, nchan, item)];
-            int z, y0;
-            group_origin(L.t, item - L.first_item, z, y0);
-            const int k = min(L.t.k, L.p.ny - y0);
-            const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
-            if (lane < Q && !*abort) {
-                const GroupRows g = group_rows_tex<ODD>(L.p, lane, y0, z, wall, L.textured);
-                if (g.bulk)
-                    copy_group<T>(L.p, L.t, g, k, stage + (size_t)lane * L.t.k * L.t.row_bytes, false, nullptr);
-                bulk_commit();
-            }
-        }
-        if (i < n) {  // load item i into the stage
-            const int item = i0 + i;
-            const ChannelLaunch &L = chans[item_channel(chans, nchan, item)];
-            int z, y0;
-            group_origin(L.t, item - L.first_item, z, y0);
-            const int k = min(L.t.k, L.p.ny - y0);
-            const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
-            GroupRows g{};
-            if (lane < Q) g = group_rows_tex<ODD>(L.p, lane, y0, z, wall, L.textured);
-            const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && g.bulk);
-            if (lane < Q) bulk_wait_read_all();  // this lane's store of the stage has read it
-            __syncwarp();
-            if (lane == 0) mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * L.t.row_bytes));
-            __syncwarp();
-            if (lane < Q && g.bulk && !*abort)
-                copy_group<T>(L.p, L.t, g, k, stage + (size_t)lane * L.t.k * L.t.row_bytes, true, full + st);
-        }
-    }
-    if (lane < Q) bulk_wait_all();
-}
-
-template <typename T, bool ODD>
-__global__ void __launch_bounds__(kTmaMaxThreads, 1)
-    step_tma_batch_kernel(const ChannelLaunch *__restrict__ chans, int nchan, const int *__restrict__ items,
-                          const int2 *__restrict__ contrib, int stages, int stage_bytes)
+__global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_batch_kernel(const ChannelLaunch *__restrict__ chans,
+                                                                           int nchan)
 {
     extern __shared__ __align__(128) unsigned char tma_smem[];
-    __shared__ int s_abort;
-    const int i0 = items[blockIdx.x], n = items[blockIdx.x + 1] - i0;
-    if (n <= 0) return;  // block-uniform; a block without items contributes to no plane
-    const int S = stages, nc = blockDim.x - 32;
-    uint64_t *full = reinterpret_cast<uint64_t *>(tma_smem + (size_t)S * stage_bytes);
-    uint64_t *empty = full + S;
+    __shared__ ChannelLaunch L;
+    __shared__ int s_c;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(full + s, 1);
-            mbar_init(empty + s, nc / 32);
-        }
-        fence_mbar_init();
-        s_abort = 0;
+        int c = 0;
+        while (c + 1 < nchan && chans[c + 1].first_block <= (int)blockIdx.x) ++c;
+        s_c = c;
     }
     __syncthreads();
-    if (threadIdx.x >= nc) {
-        batch_producer<T, ODD>(chans, nchan, i0, n, threadIdx.x - nc, tma_smem, stage_bytes, S, full, empty,
-                               &s_abort, chans[0].p.status);
-        return;
+    {
+        const int *src = reinterpret_cast<const int *>(chans + s_c);
+        int *dst = reinterpret_cast<int *>(&L);
+        for (int i = threadIdx.x; i < (int)(sizeof(ChannelLaunch) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
     }
-    double acc[NP];
-#pragma unroll
-    for (int q = 0; q < NP; ++q) acc[q] = 0.0;
-    int c = item_channel(chans, nchan, i0);
-    for (int i = 0; i < n; ++i) {
-        const int st = i % S, item = i0 + i;
-        while (c + 1 < nchan && chans[c + 1].first_item <= item) ++c;
-        const ChannelLaunch &L = chans[c];
-        const StepArgs &p = L.p;
-        const int g = item - L.first_item;
-        int z, y0;
-        group_origin(L.t, g, z, y0);
-        const int k = min(L.t.k, p.ny - y0);
-        if (!*(volatile int *)&s_abort && !mbar_wait_bounded(full + st, (uint32_t)((i / S) & 1))) {
-            s_abort = 1;
-            atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
-        }
-        const long long step = *p.step_ctr;
-        const double G = p.const_q ? p.force[step & 1] : p.gx;
-        const double *sh = p.shift + (size_t)(step & 1) * p.nz * 3 + z * 3;
-        T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
-        const int dstride = L.t.k * p.pitch;
-        const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
-#define TG(CQ, TX, W) tma_group<T, ODD, CQ, TX, W>(p, sb, dstride, y0, k, z, G, sh, acc, nc)
-#define TGW(CQ, TX) do { if (wall < 0) TG(CQ, TX, -1); else if (wall > 0) TG(CQ, TX, 1); else TG(CQ, TX, 0); } while (0)
-        if (p.const_q) {
-            if (L.textured) TGW(true, true); else TGW(true, false);
-        } else {
-            if (L.textured) TGW(false, true); else TGW(false, false);
-        }
-#undef TGW
-#undef TG
-        fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
-        __syncwarp();
-        if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);
-        const int pi = g / L.t.gpp;  // position of plane z in the channel's plane list
-        const bool plane_end = i + 1 == n || (g + 1) % L.t.gpp == 0;
-        if (plane_end) {  // this block's last group of the plane
-            const int2 ci = contrib[L.contrib + pi];
-            plane_contribute(p, acc, z, blockIdx.x - ci.x, ci.y, step, G, 0, nc);
-#pragma unroll
-            for (int q = 0; q < NP; ++q) acc[q] = 0.0;
-        }
+    __syncthreads();
+    const int blk = blockIdx.x - L.first_block;
+    const bool q = L.p.const_q != 0;
+    if (q) {
+        if (L.textured) tma_step_body<T, ODD, true, 1>(L.p, L.t, blk, tma_smem);
+        else tma_step_body<T, ODD, true, 0>(L.p, L.t, blk, tma_smem);
+    } else {
+        if (L.textured) tma_step_body<T, ODD, false, 1>(L.p, L.t, blk, tma_smem);
+        else tma_step_body<T, ODD, false, 0>(L.p, L.t, blk, tma_smem);
     }
 }
 
@@ -645,13 +533,11 @@ int tma_batch_occupancy(int threads, size_t smem)
 }
 
 template <typename T>
-void launch_tma_batch(const ChannelLaunch *chans, int nchan, const int *items, const int2 *contrib, int grid,
-                      int threads, size_t smem, int stages, int stage_bytes, bool odd, cudaStream_t s)
+void launch_tma_batch(const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem, bool odd,
+                      cudaStream_t s)
 {
-    if (odd)
-        step_tma_batch_kernel<T, true><<<grid, threads, smem, s>>>(chans, nchan, items, contrib, stages, stage_bytes);
-    else
-        step_tma_batch_kernel<T, false><<<grid, threads, smem, s>>>(chans, nchan, items, contrib, stages, stage_bytes);
+    if (odd) step_tma_batch_kernel<T, true><<<grid, threads, smem, s>>>(chans, nchan);
+    else step_tma_batch_kernel<T, false><<<grid, threads, smem, s>>>(chans, nchan);
 }
 
 }  // namespace dnslbm

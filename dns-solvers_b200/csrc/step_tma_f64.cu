@@ -14,10 +14,10 @@ void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, 
 
 int tma_batch_prepare_f64(size_t smem) { return tma_batch_set_smem_attr<double>(smem); }
 int tma_batch_occupancy_f64(int threads, size_t smem) { return tma_batch_occupancy<double>(threads, smem); }
-void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, const int *items, const int2 *contrib, int grid,
-                          int threads, size_t smem, int stages, int stage_bytes, bool odd, cudaStream_t s)
+void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem, bool odd,
+                          cudaStream_t s)
 {
-    launch_tma_batch<double>(chans, nchan, items, contrib, grid, threads, smem, stages, stage_bytes, odd, s);
+    launch_tma_batch<double>(chans, nchan, grid, threads, smem, odd, s);
 }
 
 

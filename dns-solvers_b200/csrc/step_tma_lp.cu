@@ -26,13 +26,11 @@ int tma_batch_occupancy_lp(int precision, int threads, size_t smem)
 {
     return precision == 32 ? tma_batch_occupancy<float>(threads, smem) : tma_batch_occupancy<__half>(threads, smem);
 }
-void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, const int *items,
-                         const int2 *contrib, int grid, int threads, size_t smem, int stages, int stage_bytes, bool odd,
-                         cudaStream_t s)
+void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, int grid, int threads, size_t smem,
+                         bool odd, cudaStream_t s)
 {
-    if (precision == 32)
-        launch_tma_batch<float>(chans, nchan, items, contrib, grid, threads, smem, stages, stage_bytes, odd, s);
-    else launch_tma_batch<__half>(chans, nchan, items, contrib, grid, threads, smem, stages, stage_bytes, odd, s);
+    if (precision == 32) launch_tma_batch<float>(chans, nchan, grid, threads, smem, odd, s);
+    else launch_tma_batch<__half>(chans, nchan, grid, threads, smem, odd, s);
 }
 
 
