@@ -15,7 +15,8 @@
 // force of 1e-7 per step makes visible (the bulk velocity of a long run):
 //  * u = j/rho as j - j*(drho/rho): a rounded 1/rho times rho is not 1 on
 //    average for rho just below 1 (the binade boundary), which biased the
-//    equilibrium momentum by ~3e-8 relative, ~0.6 % of the force;
+//    equilibrium momentum by ~3e-8 relative, ~0.6 % of the force; in this
+//    form the quotient's own error enters u scaled by drho ~ 1e-3;
 //  * the two momentum coefficients 3 w omega of the axis and diagonal pairs
 //    taken so that b1 + 4 b2 == omega / 2 exactly (their rounded products
 //    otherwise carry a fixed relative error of the same size).
@@ -124,7 +125,8 @@ __device__ __forceinline__ LpCell lp_collide(float (&r)[Q], float omega, float G
     LpCell c;
     c.drho = dr * iS;
     const float rho = 1.f + c.drho;
-    const float dl = c.drho * (1.f / rho);
+    // drho/rho to ~2 ulp (fast reciprocal): its error reaches u scaled by drho
+    const float dl = __fdividef(c.drho, rho);
     c.jx = jx * iS;
     const float jy_ = jy * iS, jz_ = jz * iS;
     c.u0 = fmaf(-c.jx, dl, c.jx);

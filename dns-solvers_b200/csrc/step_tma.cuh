@@ -192,18 +192,8 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
     float racc[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) racc[i] = 0.f;
-    int j = 0, x = threadIdx.x, jr = 0;
-    while (x >= nx && j < k) x -= nx, ++j;
-    for (; j < k; x += nc) {
-        while (x >= nx) x -= nx, ++j;
-        if (j >= k) break;
-        if constexpr (!std::is_same<T, double>::value) {
-            if (j != jr) {
-#pragma unroll
-                for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i], racc[i] = 0.f;
-                jr = j;
-            }
-        }
+    // one cell (row j of the group, column x)
+    auto cell = [&](int j, int x) {
         const int y = y0 + j;
         T *sbj = sb + (size_t)j * pitch;
         const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
@@ -306,6 +296,28 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
                 st_raw<T>(sbj + A * dstride + xs, v);
             }
         }
+    };
+    auto flush = [&]() {
+        if constexpr (!std::is_same<T, double>::value) {
+#pragma unroll
+            for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i], racc[i] = 0.f;
+        }
+    };
+    if (nx >= nc) {  // rows at least as long as the consumer set: row by row
+        for (int j = 0; j < k; ++j) {
+            for (int x = threadIdx.x; x < nx; x += nc) cell(j, x);
+            flush();
+        }
+        return;
+    }
+    // shorter rows: the group's k * nx cells as one range
+    int j = 0, x = threadIdx.x, jr = 0;
+    while (x >= nx && j < k) x -= nx, ++j;
+    for (; j < k; x += nc) {
+        while (x >= nx) x -= nx, ++j;
+        if (j >= k) break;
+        if (j != jr) flush(), jr = j;
+        cell(j, x);
     }
     if constexpr (!std::is_same<T, double>::value) {
 #pragma unroll
