@@ -167,6 +167,17 @@ class Dist:
             self.dist.destroy_process_group()
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(wl, seconds, steps=None, warmup=0):
     """The reference's own C step (oracle/_ref/dnsref) on this host, as
     independent single-rank processes on x-slabs of the workload; falls back
@@ -182,10 +193,17 @@ def cpu_baseline(wl, seconds, steps=None, warmup=0):
         steps = max(2, int(seconds * rate / (slab * plane)))
     else:
         slab = max(2, min(wl.nx // procs, int(seconds * rate / (steps * plane))))
+    xonly = None
     if oracle.have_reference():
         mlups, secs, procs, slab = oracle.time_reference(wl.nx, wl.ny, wl.nz, steps, warmup=warmup, omega=wl.omega,
                                                          ubulk=wl.ubulk or 0.05, procs=procs, slab=slab)
         kind = "reference"
+        try:  # xcomputations alone, a shorter sample of the same slabs
+            xonly = round(oracle.time_reference(wl.nx, wl.ny, wl.nz, max(2, steps // 2), warmup=min(warmup, 1),
+                                                omega=wl.omega, ubulk=wl.ubulk or 0.05, procs=procs, slab=slab,
+                                                only_step=True)[0], 3)
+        except Exception:  # reported as absent, never fatal
+            xonly = None
     else:
         import numpy as np
         s = np.zeros((slab, wl.ny, wl.nz + 2, 19))
@@ -197,6 +215,7 @@ def cpu_baseline(wl, seconds, steps=None, warmup=0):
         mlups = slab * plane * steps / secs / 1e6
         procs, kind = os.cpu_count() or 1, "port"
     return {"value": round(mlups, 3), "unit": "MLUPS", "cores": procs, "kind": kind,
+            "xcomputations_only_mlups": xonly, "cpu_model": _cpu_model(),
             "sample": f"{procs} independent single-rank processes x {slab}x{wl.ny}x{wl.nz} x-slab of {wl.name}, "
                       f"{steps} timed full reference steps (encalc+wshearstr+xcomputations), rest start",
             "seconds": round(secs, 3)}

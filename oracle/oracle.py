@@ -221,14 +221,16 @@ def run_reference(state, omega, ubulk=0.0, gx=0.0, const_g=True, nsteps=1, textu
         return res
 
 
-def time_reference(nx, ny, nz, nsteps, warmup=0, omega=1.9, ubulk=0.05, procs=None, slab=None, timeout=900):
+def time_reference(nx, ny, nz, nsteps, warmup=0, omega=1.9, ubulk=0.05, procs=None, slab=None, timeout=900,
+                   only_step=False):
     """CPU baseline: ``procs`` independent single-rank reference processes,
     each advancing its own x-slab (``slab`` cells of x, default nx//procs)
     of the workload as its own periodic box from the reference's rest state
     (the reference's multi-rank halo path is not usable, its neighbours are
     all itself).  Each process does ``warmup`` untimed then ``nsteps`` timed
-    full reference steps (encalc + wshearstr + xcomputations).  Returns
-    (aggregate MLUPS, slowest process seconds, procs, slab)."""
+    full reference steps (encalc + wshearstr + xcomputations), or
+    xcomputations alone with ``only_step``.  Returns (aggregate MLUPS,
+    slowest process seconds, procs, slab)."""
     procs = procs or max(1, min(os.cpu_count() or 1, nx))
     slab = slab or max(nx // procs, 2)
     with tempfile.TemporaryDirectory() as td:
@@ -238,7 +240,8 @@ def time_reference(nx, ny, nz, nsteps, warmup=0, omega=1.9, ubulk=0.05, procs=No
             os.makedirs(d)
             ps.append(subprocess.Popen([REF_BIN, f"xdv={slab}", f"ydv={ny}", f"zdv={nz}", f"omega={omega!r}",
                                         f"ubulk={ubulk!r}", "mode=q", f"steps={nsteps}", f"warmup={warmup}",
-                                        "time=1"], cwd=d, stdout=subprocess.PIPE, text=True))
+                                        "time=1", f"only_step={int(only_step)}"], cwd=d, stdout=subprocess.PIPE,
+                                       text=True))
         outs = [p.communicate(timeout=timeout)[0] for p in ps]
     if any(p.returncode for p in ps):
         raise RuntimeError("reference process failed")

@@ -31,6 +31,8 @@
  *   steps=N  stats_every=U (0: never)  vel_every=U (0: never)
  *   time=1                print timing line "MLUPS_STEP <mlups> <seconds>"
  *   warmup=W              untimed steps before the timed ones (time=1)
+ *   only_step=1           timed steps run xcomputations alone (V.force
+ *                         fixed at its first value; for timing only)
  */
 #include "definitions.h"
 #include "fun_defs.h"
@@ -72,6 +74,7 @@ int main(int argc, char **argv)
     long vel_every = atol(arg(argc, argv, "vel_every", "0"));
     int timing = atoi(arg(argc, argv, "time", "0"));
     long warmup = atol(arg(argc, argv, "warmup", "0"));
+    int only_step = atoi(arg(argc, argv, "only_step", "0"));
     int const_g = (mode[0] == 'g');
 
     int xd = xdv_ + 1, yd = ydv_ + 1, zd = zdv_ + 2;
@@ -190,9 +193,11 @@ int main(int argc, char **argv)
     double t0 = now_s();
     for (long ss = -warmup; ss < steps; ss++) {
         if (ss == 0) t0 = now_s();
-        V = encalc(xd, yd, zd, V, 0., TM, ss, ubulk, cart_grid);
-        if (const_g) V.force = gx;
-        V = wshearstr(xd, yd, zd, V, 0., omega, TM, ss, cart_grid);
+        if (!only_step || ss == -warmup) {
+            V = encalc(xd, yd, zd, V, 0., TM, ss, ubulk, cart_grid);
+            if (const_g) V.force = gx;
+            V = wshearstr(xd, yd, zd, V, 0., omega, TM, ss, cart_grid);
+        }
         if (ss >= 0 && stats_every > 0 && !(ss % stats_every)) V = statistics(xd, yd, zd, V, pd, ss / stats_every);
         if (ss >= 0 && vel_every > 0 && !(ss % vel_every)) V = vel_print(xd, yd, zd, V, ss / vel_every, cart_grid);
         if (fo && ss >= 0) {
