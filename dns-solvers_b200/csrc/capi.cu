@@ -427,19 +427,32 @@ static int initial_reduce(dnslbm_ctx *c);
 // specular reflection would land on a solid cell; the remaining links into a
 // wall plane reflect specularly and all others stream.  Solid cells keep the
 // rest state.
-static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
+// The host-side tables of a flag array: the wall-link bits of the two
+// wall-adjacent planes, the planes with link masks and the masks.  Pure host
+// computation; `err` receives the reason of a refusal.
+struct FlagTables {
+    std::vector<uint8_t> wallmask;  // [2][ny][nx]
+    std::vector<int> band;          // [nz], -1: no masks
+    std::vector<unsigned> links;    // [nband][ny][nx]
+    int nband = 0;
+    int textured = 0;  // 0 smooth walls, 1 textured walls, 2 solids inside the flow
+};
+
+static int build_flag_tables(int nx, int ny, int nz, bool general, const int8_t *fl /* [nx][ny][zd] */,
+                             FlagTables &t, char *err, size_t errlen)
 {
-    const int nx = c->nx, ny = c->ny, nz = c->nz, zd = nz + 2;
-    const bool general = c->deck.bc_mode == DNSLBM_BC_GENERAL;
+    const int zd = nz + 2;
     auto S = [&](int x, int y, int k) { return (int)fl[((size_t)x * ny + y) * zd + k]; };
     std::vector<char> has_solid(nz, 0);
     for (int x = 0; x < nx; ++x)
         for (int y = 0; y < ny; ++y) {
             for (int k : {0, zd - 1}) {
                 const int v = S(x, y, k);
-                if (v != -1 && v != -2)
-                    return fail(c, DNSLBM_ERR_ARG, "wall cell (%d,%d,%d) has flag %d; wall planes must be -1 or -2", x, y,
-                                k, v);
+                if (v != -1 && v != -2) {
+                    snprintf(err, errlen, "wall cell (%d,%d,%d) has flag %d; wall planes must be -1 or -2", x, y, k,
+                             v);
+                    return DNSLBM_ERR_ARG;
+                }
             }
             for (int k = 1; k < zd - 1; ++k) {
                 const int v = S(x, y, k);
@@ -447,21 +460,19 @@ static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
                     has_solid[k - 1] = 1;
                     continue;
                 }
-                if (v != 0 && v != 1)
-                    return fail(c, DNSLBM_ERR_ARG,
-                                general ? "cell (%d,%d,%d) has flag %d; inside the flow a cell is fluid (0, 1) or solid (-1)"
-                                        : "cell (%d,%d,%d) has flag %d; solids inside the flow need the general boundary "
-                                          "mode (DNSLBM_BC_GENERAL)",
-                                x, y, k, v);
+                if (v != 0 && v != 1) {
+                    snprintf(err, errlen,
+                             general ? "cell (%d,%d,%d) has flag %d; inside the flow a cell is fluid (0, 1) or solid (-1)"
+                                     : "cell (%d,%d,%d) has flag %d; solids inside the flow need the general boundary "
+                                       "mode (DNSLBM_BC_GENERAL)",
+                             x, y, k, v);
+                    return DNSLBM_ERR_ARG;
+                }
             }
         }
-    if (c->have_state && c->odd) {
-        // the populations in flight were placed under the old flags
-        return fail(c, DNSLBM_ERR_STATE, "flags can only change between even numbers of steps");
-    }
-    std::vector<uint8_t> m((size_t)2 * nx * ny);
+    t.wallmask.assign((size_t)2 * nx * ny, 0);
     const int off[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
-    int textured = 0;
+    t.textured = 0;
     for (int w = 0; w < 2; ++w) {
         const int k = w == 0 ? 0 : zd - 1;
         for (int y = 0; y < ny; ++y)
@@ -471,18 +482,18 @@ static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
                     const int xt = (x + off[l][0] + nx) % nx, yt = (y + off[l][1] + ny) % ny;
                     if (S(xt, yt, k) == -1 && S(x, y, k) == -1) bits |= 1u << l;
                 }
-                m[(size_t)w * nx * ny + (size_t)y * nx + x] = (uint8_t)bits;
-                if (bits != 0x1f) textured = 1;
+                t.wallmask[(size_t)w * nx * ny + (size_t)y * nx + x] = (uint8_t)bits;
+                if (bits != 0x1f) t.textured = 1;
             }
     }
     // planes with link masks
-    std::vector<int> band(nz, -1);
-    int nband = 0;
+    t.band.assign(nz, -1);
+    t.nband = 0;
     for (int z = 0; z < nz; ++z)
-        if (has_solid[z] || (z > 0 && has_solid[z - 1]) || (z + 1 < nz && has_solid[z + 1])) band[z] = nband++;
-    std::vector<unsigned> lk((size_t)nband * ny * nx, 0u);
+        if (has_solid[z] || (z > 0 && has_solid[z - 1]) || (z + 1 < nz && has_solid[z + 1])) t.band[z] = t.nband++;
+    t.links.assign((size_t)t.nband * ny * nx, 0u);
     for (int z = 0; z < nz; ++z) {
-        if (band[z] < 0) continue;
+        if (t.band[z] < 0) continue;
         const int k = z + 1;
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) {
@@ -501,10 +512,46 @@ static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
                         if (bounce) v |= 1u << a;
                     }
                 }
-                lk[((size_t)band[z] * ny + y) * nx + x] = v;
+                t.links[((size_t)t.band[z] * ny + y) * nx + x] = v;
             }
     }
-    if (nband > 0) textured = 2;
+    if (t.nband > 0) t.textured = 2;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_link_masks(int xdv, int ydv, int zdv, int bc_mode, const int8_t *flags, int *band_of,
+                                 unsigned *links, size_t links_capacity, int *nband)
+{
+    dnslbm_ctx *c = nullptr;
+    if (!flags || !band_of || !nband || xdv < 1 || ydv < 1 || zdv < 1)
+        return fail(c, DNSLBM_ERR_ARG, "bad grid or null argument");
+    FlagTables t;
+    char err[256];
+    int rc = build_flag_tables(xdv, ydv, zdv, bc_mode == DNSLBM_BC_GENERAL, flags, t, err, sizeof err);
+    if (rc) return fail(c, rc, "%s", err);
+    *nband = t.nband;
+    for (int z = 0; z < zdv; ++z) band_of[z] = t.band[z];
+    if (t.links.size() > links_capacity || (!links && !t.links.empty()))
+        return fail(c, DNSLBM_ERR_ARG, "link masks need %zu entries, %zu given", t.links.size(), links_capacity);
+    std::copy(t.links.begin(), t.links.end(), links);
+    return DNSLBM_OK;
+}
+
+static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    FlagTables t;
+    char err[256];
+    const int brc = build_flag_tables(nx, ny, nz, c->deck.bc_mode == DNSLBM_BC_GENERAL, fl, t, err, sizeof err);
+    if (brc) return fail(c, brc, "%s", err);
+    if (c->have_state && c->odd) {
+        // the populations in flight were placed under the old flags
+        return fail(c, DNSLBM_ERR_STATE, "flags can only change between even numbers of steps");
+    }
+    std::vector<uint8_t> &m = t.wallmask;
+    std::vector<int> &band = t.band;
+    std::vector<unsigned> &lk = t.links;
+    const int nband = t.nband, textured = t.textured;
     CK(cudaSetDevice(c->deck.device));
     const size_t lbytes = lk.size() * sizeof(unsigned);
     if (lbytes > c->links_bytes) {

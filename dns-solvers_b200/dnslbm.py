@@ -60,6 +60,8 @@ def lib():
     L.dnslbm_last_error.restype = ctypes.c_char_p
     L.dnslbm_set_flags.argtypes = [vp, ip]
     L.dnslbm_set_flags_periodic.argtypes = [vp, i8p]
+    L.dnslbm_link_masks.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, i8p, ip,
+                                    ctypes.POINTER(ctypes.c_uint), ctypes.c_size_t, ip]
     L.dnslbm_init_rest.argtypes = [vp]
     L.dnslbm_load_state.argtypes = [vp, dp]
     L.dnslbm_store_state.argtypes = [vp, dp]
@@ -319,6 +321,23 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+
+def link_masks(flags, bc_mode=BC_GENERAL):
+    """(band_of [zdv], links [nband, ydv, xdv]) the library builds from an
+    int8 (xdv, ydv, zdv+2) flag array (host only, dnslbm_link_masks)."""
+    L = lib()
+    f = np.ascontiguousarray(flags, np.int8)
+    nx, ny, zd = f.shape
+    band = np.zeros(zd - 2, np.int32)
+    links = np.zeros((zd - 2) * ny * nx, np.uint32)
+    nb = ctypes.c_int()
+    rc = L.dnslbm_link_masks(nx, ny, zd - 2, bc_mode, f.ctypes.data_as(ctypes.POINTER(ctypes.c_int8)),
+                             band.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             links.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), links.size, ctypes.byref(nb))
+    if rc:
+        raise DnsLbmError(rc, L.dnslbm_last_error(None).decode())
+    return band, links[:nb.value * ny * nx].reshape(nb.value, ny, nx)
 
 
 class PinnedArray:

@@ -109,6 +109,15 @@ int dnslbm_set_flags(dnslbm_ctx *ctx, const int *s);
  * the plane sums like any other cell.  Wall planes are -1 or -2 in either
  * mode; flags change only between even numbers of steps. */
 int dnslbm_set_flags_periodic(dnslbm_ctx *ctx, const int8_t *flags);
+/* Host only (no device is touched): the per-cell link masks that
+ * dnslbm_set_flags_periodic builds from `flags` for boundary mode
+ * `bc_mode`: band_of[zdv] gets each fluid plane's mask block (-1: none),
+ * links[nband][ydv][xdv] the masks (bit 0 solid, bit A: link A bounces
+ * back), nband the number of blocks.  A diagnostic of the wall rule; no
+ * counterpart in the reference.  DNSLBM_ERR_ARG for invalid flags or a
+ * links_capacity (entries) below nband * ydv * xdv. */
+int dnslbm_link_masks(int xdv, int ydv, int zdv, int bc_mode, const int8_t *flags, int *band_of, unsigned *links,
+                      size_t links_capacity, int *nband);
 
 /* Initial state: rest, f = w (init.c:6-19). */
 int dnslbm_init_rest(dnslbm_ctx *ctx);

@@ -7,7 +7,10 @@ GPU-vs-oracle parity tests the rule itself is checked here.
     fluid populations is unchanged (no population lost or duplicated), for
     riblets and for blocks standing on slip-grooved walls.
   * Mass is conserved over many collide-and-stream steps, and solid cells
-    keep their rest populations."""
+    keep their rest populations.
+  * The per-cell link masks the library builds on the host
+    (dnslbm_link_masks, used by dnslbm_set_flags) follow the same rule,
+    written once more in numpy here."""
 import numpy as np
 import pytest
 
@@ -64,3 +67,55 @@ def test_mass_conserved_and_solids_at_rest(oracle_mod, kind):
     oracle_mod.run(st, fl, 1.8, gx=3e-5, const_g=True, nsteps=30, bc_mode=1)
     assert abs(st[:, :, 1:-1].sum() - m0) < 1e-11 * m0
     assert np.all(st[:, :, 1:-1][~fluid(fl)] == inputs.W)
+
+
+def link_masks_restated(flags):
+    """The general wall rule, written once more in numpy: for every fluid
+    cell of a plane within one plane of a solid, bit A set when the link in
+    direction A bounces back (lbm_oracle.c orc_step_ab, bc_mode 1)."""
+    nx, ny, zd = flags.shape
+    nz = zd - 2
+    solid = (flags[:, :, 1:-1] == -1).any(axis=(0, 1))
+    band = -np.ones(nz, int)
+    nb = 0
+    for z in range(nz):
+        if solid[max(z - 1, 0):z + 2].any():
+            band[z] = nb
+            nb += 1
+    E = inputs.E.astype(int)
+    out = np.zeros((nb, ny, nx), np.uint32)
+    X, Y = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    for z in range(nz):
+        if band[z] < 0:
+            continue
+        k = z + 1
+        v = np.zeros((nx, ny), np.uint32)
+        for a in range(1, 19):
+            xt, yt, kt = (X + E[a, 0]) % nx, (Y + E[a, 1]) % ny, k + E[a, 2]
+            sld, sld1, sdest = flags[xt, yt, kt], flags[X, Y, kt], flags[xt, yt, k]
+            spec = ((sld == -1) & (sld1 == -2)) | (sld == -2)
+            bounce = np.where(sld > -1, False, np.where((sld == -1) & (sld1 == -1), True,
+                                                         np.where(spec, sdest == -1, True)))
+            v |= (bounce.astype(np.uint32) << a)
+        v[flags[:, :, k] == -1] = 1
+        out[band[z]] = v.T
+    return band, out
+
+
+@pytest.mark.parametrize("kind", ["riblets", "blocks", "grooves only"])
+def test_library_link_masks_follow_the_rule(kind):
+    import dnslbm
+    nx, ny, nz = 20, 16, 12
+    fl = {"riblets": lambda: inputs.flags_riblets(nx, ny, nz, 4, 8),
+          "blocks": lambda: blocks_on_grooves(nx, ny, nz, 5),
+          "grooves only": lambda: inputs.flags_longitudinal(nx, ny, nz, 3, 3)}[kind]()
+    band, links = dnslbm.link_masks(fl)
+    rband, rlinks = link_masks_restated(fl)
+    np.testing.assert_array_equal(band, rband)
+    np.testing.assert_array_equal(links, rlinks)
+    if kind == "grooves only":
+        assert links.size == 0
+    else:
+        with pytest.raises(dnslbm.DnsLbmError) as e:
+            dnslbm.link_masks(fl, bc_mode=dnslbm.BC_REFERENCE)
+        assert "DNSLBM_BC_GENERAL" in str(e.value)
