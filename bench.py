@@ -454,7 +454,7 @@ def run_ours(args):
                            "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU",
                            "l2": f"state {cells * 19 * args.precision / 8 / 1e9:.2f} GB vs 126 MB L2, no flush"},
                 "roofline": roof, "variants": variants, "batched": batched, "e2e": e2e, "cpu_baseline": cb,
-                "gpu_launches": args.steps, "clocks": clk.summary()}
+                "gpu_launches": args.steps * (2 if "links_pass_kernel" in kdesc else 1), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     ch.close()
     d.close()
