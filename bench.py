@@ -240,6 +240,31 @@ def run_reference_arm(args):
     d.close()
 
 
+def parity_fracs(bpc, cells, ms_even, ms_odd, n_even, n_odd, peak):
+    """Roofline fraction of the even- and odd-parity step launches (mean
+    launch time of each)."""
+    def frac(ms, n):
+        return round(bpc * cells / (ms / n / 1e3) / 1e9 / peak, 4) if n and ms > 0 else None
+    return frac(ms_even, n_even), frac(ms_odd, n_odd)
+
+
+def variant_summary(v):
+    r, e = v["roofline"], v["error_vs_f64"]
+    return {"value": v["value"], "unit": "MLUPS", "ms_per_step": v["ms_per_step"], "speedup_vs_f64": v["speedup_vs_f64"],
+            "frac_even": r["frac_even"], "frac_odd": r["frac_odd"], "whole_step_frac": r["whole_step_frac"],
+            "err_mean_u": float(f"{e['mean_u_profile_max_rel']:.3g}"),
+            "err_u_rms": float(f"{e['u_rms_profile_max_rel']:.3g}"), "err_after_steps": e["after_steps"]}
+
+
+def batched_summary(b):
+    if "error" in b:
+        return b
+    return {"channels": b["channels"], "seed": b["seed"], "cells": b["cells"], "dtype": b["dtype"],
+            "value": b["value"], "ms_per_step": b["ms_per_step"], "one_at_a_time": b["one_at_a_time"]["value"],
+            "speedup_vs_one_at_a_time": b["speedup_vs_one_at_a_time"],
+            "whole_step_frac": b["whole_step_frac_of_hbm"], "kernel": b["kernel_config"].split(":")[0]}
+
+
 def timed_run(ch, steps, warmup):
     if warmup:
         ch.step_timed(warmup)
@@ -294,14 +319,14 @@ def batched_report(args, dev):
     return {"workload": "24 channels, h in {20, 32, 48, 64}, (2 pi h) x (2h + 2) x (pi h), seeded walls "
                         "(smooth / longitudinal grooves / transverse grooves / triangular riblets), Re_tau in "
                         "[120, 180]",
-            "channels": [w.name for w in chans], "cells": cells, "dtype": "f32", "steps": args.steps,
+            "channels": len(chans), "seed": 0, "cells": cells, "dtype": "f32", "steps": args.steps,
             "value": round(cells * args.steps / (ms_b / 1e3) / 1e6, 1), "unit": "MLUPS",
             "ms_per_step": round(ms_b / args.steps, 4),
             "one_at_a_time": {"value": round(cells * args.steps / (ms_alone / 1e3) / 1e6, 1), "unit": "MLUPS",
                               "ms_per_step": round(ms_alone / args.steps, 4)},
             "speedup_vs_one_at_a_time": round(ms_alone / ms_b, 3),
             "whole_step_frac_of_hbm": round(bpc * cells / (ms_b / args.steps / 1e3) / 1e9 / peak, 4),
-            "kernel_config": kdesc, "autotune": tune}
+            "kernel_config": kdesc}
 
 
 def run_ours(args):
@@ -358,9 +383,11 @@ def run_ours(args):
     launch_s = kms / kn / 1e3
     achieved = bpc * cells / launch_s / 1e9
     traffic = ncu_traffic(f"{wl.name}:f{args.precision}")
+    fe, fo = parity_fracs(bpc, cells, even, odd, n_even, n_odd, peak)
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": f"{peak_src} (MEASURED_PEAKS.json)",
             "kernel": kname, "kernel_config": kdesc, "autotune": tune, "launch_ms": round(launch_s * 1e3, 4),
+            "frac_even": fe, "frac_odd": fo,
             "whole_step_frac": round(bpc * cells / (tmax / args.steps / 1e3) / 1e9 / peak, 4),
             "algorithmic_bytes_per_launch": bpc * cells, "bytes_per_cell": bpc}
 
@@ -383,13 +410,14 @@ def run_ours(args):
             b2 = c2.bytes_per_cell
             k2 = max(e2, o2) / (n_odd if o2 >= e2 else n_even) / 1e3
             ach2 = b2 * cells / k2 / 1e9
+            fe2, fo2 = parity_fracs(b2, cells, e2, o2, n_even, n_odd, peak)
             um_ref, um = ref_stats[0, 1:-1], st[0, 1:-1]
             urms_ref, urms = ref_stats[3, 1:-1], st[3, 1:-1]
             variants[f"f{prec}"] = {
                 "value": round(cells * args.steps / (t2 / 1e3) / 1e6, 1), "unit": "MLUPS",
                 "ms_per_step": round(t2 / args.steps, 4), "speedup_vs_f64": round(tot / t2, 3),
                 "roofline": {"bound": "hbm", "achieved": round(ach2, 1), "peak": peak, "unit": "GB/s",
-                             "frac": round(ach2 / peak, 4), "bytes_per_cell": b2,
+                             "frac": round(ach2 / peak, 4), "frac_even": fe2, "frac_odd": fo2, "bytes_per_cell": b2,
                              "whole_step_frac": round(b2 * cells / (t2 / args.steps / 1e3) / 1e9 / peak, 4),
                              "traffic": ncu_traffic(f"{wl.name}:f{prec}"), "kernel_config": c2.kernel,
                              "autotune": tune2},
@@ -453,8 +481,13 @@ def run_ours(args):
                            "walls": wl.texture, "force": f"constant g={wl.gx:.3e}", "omega": wl.omega,
                            "parallelism": f"replicas x{d.world}" if d.world > 1 else "single GPU",
                            "l2": f"state {cells * 19 * args.precision / 8 / 1e9:.2f} GB vs 126 MB L2, no flush"},
-                "roofline": roof, "variants": variants, "batched": batched, "e2e": e2e, "cpu_baseline": cb,
+                "variants": variants, "roofline": roof, "e2e": e2e, "cpu_baseline": cb,
                 "gpu_launches": args.steps * (2 if "links_pass_kernel" in kdesc else 1), "clocks": clk.summary()}
+        # short summaries last, so that a reader of the line's tail sees them
+        if batched is not None:
+            line["batched"] = batched_summary(batched)
+        for k, v in variants.items():
+            line[f"{k}_storage"] = variant_summary(v)
         print(json.dumps(line), flush=True)
     ch.close()
     d.close()

@@ -28,6 +28,7 @@
 namespace dnslbm {
 void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex, cudaStream_t s);
 void launch_reduce_f64(const StepArgs &p, dim3 grid, dim3 block, cudaStream_t s);
+void launch_reduce_f64_odd(const StepArgs &p, dim3 grid, dim3 block, int tex, cudaStream_t s);
 }  // namespace dnslbm
 
 using namespace dnslbm;
@@ -172,9 +173,11 @@ extern "C" int dnslbm_step_f64_noalloc(double *pop, size_t pop_stride, int xdv, 
 
     const dim3 block(bx, 1, 1), grid((xdv + bx - 1) / bx, (ydv + rows - 1) / rows, zdv);
     noalloc_reset_kernel<<<64, 256, 0, s>>>(scratch, L, zdv, gx);
-    // a state in the natural layout gets the plane means of the first step,
-    // exactly as after dnslbm_load_state
+    // the plane means of the state the first step starts from (the shift of
+    // the one-pass energy sum), as after dnslbm_load_state; a state left by
+    // an odd number of steps is read through the odd-step address set
     if (parity == 0) launch_reduce_f64(p, grid, block, s);
+    else launch_reduce_f64_odd(p, grid, block, wallmask != nullptr ? 1 : 0, s);
     for (long n = 0; n < nsteps; ++n)
         launch_step_f64(p, grid, block, ((parity + n) & 1) != 0, wallmask != nullptr ? 1 : 0, s);
     e = cudaGetLastError();

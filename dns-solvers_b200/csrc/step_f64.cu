@@ -136,6 +136,53 @@ __global__ void __launch_bounds__(128) reduce_f64_kernel(const StepArgs p)
     block_epilogue(p, acc, step, 0.0, 1);
 }
 
+// The same for a state left by an odd number of steps (post-collision
+// values in swapped slots): each cell gathers its populations through the
+// odd-step address set (periodic wrap, wall links by the wall mask), so the
+// sums are those of the state the next step starts from.  Used by the
+// allocation-free entry point, which has no plane means carried over from an
+// earlier call.
+template <int TEX>
+__global__ void __launch_bounds__(128) reduce_f64_odd_kernel(const StepArgs p)
+{
+    const long long step = *p.step_ctr;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.z;
+    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    double acc[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) acc[i] = 0.0;
+    if (x < p.nx) {
+        const int y0 = blockIdx.y * p.rows;
+        const int y1 = min(y0 + p.rows, p.ny);
+        for (int y = y0; y < y1; ++y) {
+            const Nbr n = make_nbr(x, y, z, p.nx, p.ny, p.pitch);
+            unsigned bits = 0x1fu;
+            if (TEX != 0 && wall != 0) bits = p.wallmask[(size_t)(wall > 0) * p.nx * p.ny + y * p.nx + x];
+            double f[Q];
+#pragma unroll
+            for (int a = 0; a < Q; ++a) {
+                const double *q;
+                switch (a) {
+#define PT(A) case A: q = f64_ptr<A, true>(p, n, wall, bits); break;
+                    PT(0) PT(1) PT(2) PT(3) PT(4) PT(5) PT(6) PT(7) PT(8) PT(9)
+                    PT(10) PT(11) PT(12) PT(13) PT(14) PT(15) PT(16) PT(17) PT(18)
+#undef PT
+                }
+                f[lat_opp(a)] = *q;
+            }
+            double dens, jx, jy, jz;
+            f64_moments(f, dens, jx, jy, jz);
+            acc[0] += dens;
+            acc[1] += jx;
+            acc[2] += jx / dens;
+            acc[3] += jy / dens;
+            acc[4] += jz / dens;
+        }
+    }
+    block_epilogue(p, acc, step, 0.0, 1);
+}
+
 void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex, cudaStream_t s)
 {
     const bool q = p.const_q != 0;
@@ -153,6 +200,12 @@ void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex
 void launch_reduce_f64(const StepArgs &p, dim3 grid, dim3 block, cudaStream_t s)
 {
     reduce_f64_kernel<<<grid, block, 0, s>>>(p);
+}
+
+void launch_reduce_f64_odd(const StepArgs &p, dim3 grid, dim3 block, int tex, cudaStream_t s)
+{
+    if (tex) reduce_f64_odd_kernel<1><<<grid, block, 0, s>>>(p);
+    else reduce_f64_odd_kernel<0><<<grid, block, 0, s>>>(p);
 }
 
 }  // namespace dnslbm

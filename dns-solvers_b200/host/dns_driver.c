@@ -22,7 +22,7 @@
  *
  * Files written (formats of the reference):
  *   energy.txt flowrate.txt massrate.txt   encalc.c:125-138, every step
- *   str-up.txt str-do.txt w-str.txt p-grad.txt   wshearstr.c:278-300
+ *   str-up.txt str-do.txt w-str.txt p-grad.txt   wshearstr.c:133-154
  *   lbf.NNNN force.NNNN   every 10*utime steps, dns-const-q-xycut.c:491-513
  *   vel.NNNN den.NNNN     every utime steps, vel_print.c
  *   turb-fld.000.TTT uavg-temp.dat   every utime steps, statistics.c:135-165

@@ -15,7 +15,7 @@ size of FP32 rounding (amp 1e-7); an FP32/FP16 error at the level of the
 control's is the flow's sensitivity, not a precision bias.
 
 Averaged over the window (after --spinup steps), per run:
-  * the per-step wall shear stress (wshearstr.c:271) -> u_tau = sqrt(tau_w/rho),
+  * the per-step wall shear stress (wshearstr.c:125) -> u_tau = sqrt(tau_w/rho),
     Re_tau = u_tau h / nu (h = zdv/2, nu = (2/omega - 1)/6);
   * the flow rate (encalc.c:132) -> bulk velocity and skin friction
     C_f = 2 tau_w / (rho U_b^2);

@@ -66,10 +66,10 @@ extern "C" {
 #define DNSLBM_LOG_ENERGY 2   /* K (encalc.c:106-114) -> energy.txt             */
 #define DNSLBM_LOG_FLOWRATE 3 /* U*(ydv*zdv) (encalc.c:132) -> flowrate.txt     */
 #define DNSLBM_LOG_MASSRATE 4 /* mean jx*(ydv*zdv) (encalc.c:136) -> massrate.txt */
-#define DNSLBM_LOG_STUP 5     /* wshearstr.c:250-269 -> str-up.txt              */
-#define DNSLBM_LOG_STDOWN 6   /* wshearstr.c:203-216 -> str-do.txt              */
-#define DNSLBM_LOG_STRESS 7   /* wshearstr.c:271 -> w-str.txt                   */
-#define DNSLBM_LOG_PGRAD 8    /* wshearstr.c:265-267 -> p-grad.txt              */
+#define DNSLBM_LOG_STUP 5     /* wshearstr.c:72-123 -> str-up.txt               */
+#define DNSLBM_LOG_STDOWN 6   /* wshearstr.c:26-70 -> str-do.txt                */
+#define DNSLBM_LOG_STRESS 7   /* wshearstr.c:125 -> w-str.txt                   */
+#define DNSLBM_LOG_PGRAD 8    /* wshearstr.c:119-121 -> p-grad.txt              */
 #define DNSLBM_LOG_N 9
 
 /* The parameter deck.  Replaces the compile-time #defines of

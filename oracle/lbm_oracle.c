@@ -214,7 +214,7 @@ int orc_wshearstr(int nx, int ny, int nz, const double *state, double omega, dou
         }
     davg /= ((double)(nx * ny));
     stup /= ((double)(nx * ny));
-    double pgrad = force * (zd - 2) / 2.; /* wshearstr.c:265-267 */
+    double pgrad = force * (zd - 2) / 2.; /* wshearstr.c:119-121 */
     stup *= mu * davg;
     double stress = 0.5 * (stup + stdown);
     if (out) {

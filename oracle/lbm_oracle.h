@@ -30,10 +30,10 @@ enum {
     ORC_LOG_ENERGY,      /* K, encalc.c:106-114 (energy.txt)                  */
     ORC_LOG_FLOWRATE,    /* U*(ny*nz), encalc.c:116-119,132 (flowrate.txt)    */
     ORC_LOG_MASSRATE,    /* momentum*(ny*nz), encalc.c:136 (massrate.txt)     */
-    ORC_LOG_STUP,        /* wshearstr.c:250-269 (str-up.txt)                  */
-    ORC_LOG_STDOWN,      /* wshearstr.c:203-216 (str-do.txt)                  */
-    ORC_LOG_STRESS,      /* wshearstr.c:271 (w-str.txt)                       */
-    ORC_LOG_PGRAD,       /* wshearstr.c:265-267 (p-grad.txt)                  */
+    ORC_LOG_STUP,        /* wshearstr.c:72-123 (str-up.txt)                   */
+    ORC_LOG_STDOWN,      /* wshearstr.c:26-70 (str-do.txt)                    */
+    ORC_LOG_STRESS,      /* wshearstr.c:125 (w-str.txt)                       */
+    ORC_LOG_PGRAD,       /* wshearstr.c:119-121 (p-grad.txt)                  */
     ORC_LOG_N
 };
 

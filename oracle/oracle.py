@@ -24,6 +24,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblbmoracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "dnsref")
+# the reference's DNS-solver/src directory (the one place it is named; the
+# Makefile's REF_SRC gets the same value)
+REF_SRC = os.environ.get("REF_SRC", "/root/reference/DNS-solver/src")
 
 LOG_NAMES = ("force", "rho", "energy", "flowrate", "massrate", "stup", "stdown", "stress", "pgrad")
 NLOG = len(LOG_NAMES)
@@ -36,8 +39,12 @@ def build(quiet: bool = True) -> None:
     reference sources are present on this machine)."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=out)
-    if os.path.isdir("/root/reference/DNS-solver/src"):
-        subprocess.run(["make", "-C", HERE, "ref"], check=True, stdout=out)
+    if have_reference_sources():
+        subprocess.run(["make", "-C", HERE, "ref", f"REF_SRC={REF_SRC}"], check=True, stdout=out)
+
+
+def have_reference_sources() -> bool:
+    return os.path.isdir(REF_SRC)
 
 
 def lib():

@@ -6,7 +6,7 @@ stores inputs, final states, per-step force/density and the parsed text logs
 (energy.txt, flowrate.txt, massrate.txt, str-up.txt, str-do.txt, w-str.txt,
 p-grad.txt) and statistics (turb-fld) / vel / den outputs as npz files.
 
-    python tests/golden/make_golden.py      (needs /root/reference; run once)
+    python tests/golden/make_golden.py      (needs the reference sources at $REF_SRC; run once)
 """
 import os
 import sys

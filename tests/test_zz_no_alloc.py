@@ -4,19 +4,26 @@ A host code that hands out all device memory from its own pool cannot let a
 library call cudaMalloc; it keeps the populations in its own device buffer and
 calls dnslbm_step_f64_noalloc, whose scratch is a static device array.  This
 test drives that entry point through the C ABI on caller-owned buffers (made
-here with torch) and checks it against the context entry point
-(dnslbm_create / dnslbm_load_state / dnslbm_step) on the same input, over two
-calls in a row: FP64 populations bit for bit, log records within the 1e-11
-relative tolerance used for FP64 logs elsewhere.  Collected last so a failure
-here does not hide the other tests.
+here with torch) and checks it, over two calls in a row, against the context
+entry point (dnslbm_create / dnslbm_load_state / dnslbm_step) on the same
+input and against the CPU oracle: FP64 populations bit for bit, log records
+within the 1e-11 relative tolerance used for FP64 logs elsewhere.  Odd call
+lengths make the second call start from a state left by an odd number of
+steps (parity 1).  Collected last so a failure here does not hide the other
+tests.
 """
 import ctypes
+import os
+import sys
 
 import numpy as np
 import pytest
 
 import dnslbm
 import inputs
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import oracle  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -46,8 +53,9 @@ def from_soa(soa, shape):
     return s
 
 
+@pytest.mark.parametrize("calls", [(4, 6), (3, 5)])
 @pytest.mark.parametrize("textured", [False, True])
-def test_noalloc_matches_context_entry_point(textured):
+def test_noalloc_matches_context_entry_point(textured, calls):
     torch = pytest.importorskip("torch")
     L = dnslbm.lib()
     L.dnslbm_step_f64_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
@@ -57,7 +65,9 @@ def test_noalloc_matches_context_entry_point(textured):
     nx, ny, nz, omega, gx = 40, 24, 12, 1.75, 3e-5
     flags = inputs.flags_longitudinal(nx, ny, nz, 3, 3) if textured else inputs.flags_smooth(nx, ny, nz)
     s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 21)
-    calls = (4, 6)  # two calls in a row; even counts leave the natural layout
+    # two calls in a row; an odd first call leaves the second one a state in
+    # the swapped (parity 1) layout, and the sum is even, so the final state
+    # is in the natural layout
 
     with dnslbm.Channel(nx, ny, nz, omega, gx=gx, force_mode=dnslbm.CONST_G, precision=64) as ch:
         ch.set_flags(flags)
@@ -83,8 +93,14 @@ def test_noalloc_matches_context_entry_point(textured):
         parity = (parity + n) % 2
         got_logs.append(logs.cpu().numpy())
     got_state = from_soa(pop.cpu().numpy(), s0.shape)
+    got_logs = np.concatenate(got_logs)
     np.testing.assert_array_equal(got_state, want_state)
-    np.testing.assert_allclose(np.concatenate(got_logs), want_logs, rtol=1e-11, atol=1e-15)
+    np.testing.assert_allclose(got_logs, want_logs, rtol=1e-11, atol=1e-15)
+
+    ref = s0.copy()
+    ref_logs = oracle.run(ref, flags, omega, gx=gx, const_g=True, nsteps=sum(calls))
+    np.testing.assert_array_equal(got_state, ref)
+    np.testing.assert_allclose(got_logs, ref_logs, rtol=1e-11, atol=1e-15)
 
 
 def test_noalloc_rejects_oversized_grid():
