@@ -87,6 +87,8 @@ struct dnslbm_ctx {
     size_t tma_smem = 0;
     TmaArgs tma{};
     int have_state = 0;
+    unsigned long long wait_ns = 1000000000ull;  // limit of a bounded device wait (1 s)
+    int withhold = 0;                            // test hook: the next bulk-copy launch withholds a load
     int odd = 0;  // parity of the next step (1: populations are post-collision, swapped)
     long long done = 0;
     int slab_next = 0;  // next x of a state loaded in slabs
@@ -138,6 +140,8 @@ static StepArgs step_args(const dnslbm_ctx *c)
     p.status = c->status;
     p.band_of = c->band_of;
     p.links = c->links;
+    p.wait_ns = c->wait_ns;
+    p.withhold_stage = 0;
     return p;
 }
 
@@ -739,6 +743,12 @@ static int launch_steps(dnslbm_ctx *c, long n, bool timed, double *ms_even, doub
         const bool odd = c->odd != 0;
         if (timed) CK(cudaEventRecord(c->tev[2 * s], c->stream));
         if (c->use_tma) {
+            if (c->withhold && c->tma.ngroups > 0) {  // test hook, one launch only
+                p.withhold_stage = 1;
+                c->withhold = 0;
+            } else {
+                p.withhold_stage = 0;
+            }
             // the row-pipelined kernel over its planes and, beside it on a
             // second stream, the planes with link masks per cell (disjoint
             // addresses; whichever finishes the last plane runs the step tail)
@@ -791,7 +801,10 @@ static int check_status(dnslbm_ctx *c)
     long long st[2];
     CK(cudaMemcpyAsync(st, c->status, sizeof st, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    if (st[1]) return fail(c, DNSLBM_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out; state invalid, reload it");
+    if (st[1]) {
+        c->have_state = 0;  // blocks that gave up left their rows unstepped
+        return fail(c, DNSLBM_ERR_TIMEOUT, "a bounded wait for a bulk copy ran out; state invalid, reload it");
+    }
     if (st[0]) return fail(c, DNSLBM_ERR_NAN, "NaN wall shear stress at step %lld", st[0] - 1);
     return DNSLBM_OK;
 }
@@ -823,6 +836,23 @@ extern "C" int dnslbm_step_timed(dnslbm_ctx *c, long nsteps, double *ms_total, d
     CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
     *ms_total = ms;
     return check_status(c);
+}
+
+extern "C" int dnslbm_set_wait_limit(dnslbm_ctx *c, double ms)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!(ms > 0.0 && ms <= 600000.0)) return fail(c, DNSLBM_ERR_ARG, "wait limit %g ms outside (0, 600000]", ms);
+    c->wait_ns = (unsigned long long)(ms * 1e6);
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_test_withhold_load(dnslbm_ctx *c)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->use_tma || c->tma.ngroups <= 0)
+        return fail(c, DNSLBM_ERR_STATE, "the context steps with a kernel that has no bounded waits");
+    c->withhold = 1;
+    return DNSLBM_OK;
 }
 
 extern "C" long dnslbm_steps_done(const dnslbm_ctx *c) { return c ? (long)c->done : -1; }

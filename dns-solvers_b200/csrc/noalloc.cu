@@ -170,6 +170,8 @@ extern "C" int dnslbm_step_f64_noalloc(double *pop, size_t pop_stride, int xdv, 
     p.logs = logs ? logs : scratch + L.logs;
     p.log_cap = logs ? (int)(nsteps < 0x7fffffffL ? nsteps : 0x7fffffffL) : 1;
     p.status = reinterpret_cast<long long *>(scratch + L.status);
+    p.wait_ns = 1000000000ull;  // the per-thread kernel has no bounded waits
+    p.withhold_stage = 0;
 
     const dim3 block(bx, 1, 1), grid((xdv + bx - 1) / bx, (ydv + rows - 1) / rows, zdv);
     noalloc_reset_kernel<<<64, 256, 0, s>>>(scratch, L, zdv, gx);

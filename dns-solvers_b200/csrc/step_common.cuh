@@ -37,11 +37,16 @@ struct StepArgs {
     unsigned *total_ctr;     // [1]
     double *logs;            // [log_cap][9]
     int log_cap;
-    long long *status;       // [0] first NaN step + 1 (0: none)
+    long long *status;       // [0] first NaN step + 1 (0: none), [1] a bounded wait gave up
     // solids inside the flow (general boundary mode): planes within one
     // plane of a solid cell carry a per-cell link mask, see cell_links
     const int *band_of;      // [nz] index of the plane's mask block, -1: none
     const unsigned *links;   // [nband][ny][nx]
+    // bounded waits of the row-pipelined kernels: a wait gives up after
+    // wait_ns of the GPU's global timer (status[1] set); withhold_stage is a
+    // test switch (0 otherwise) that makes one block withhold a load
+    unsigned long long wait_ns;
+    int withhold_stage;
 };
 
 // Arguments of the state readers/writers (import, export, moments, stats).

@@ -29,9 +29,11 @@
 //
 // TEX: 0 smooth walls, 1 textured walls.
 //
-// Every wait on an mbarrier is bounded; a wait that runs out records
-// status[1] and a shared abort flag, after which no thread of the block waits
-// again (the host reports DNSLBM_ERR_TIMEOUT).
+// Every wait on an mbarrier is bounded in time (StepArgs::wait_ns of the
+// GPU's global timer); a wait that runs out records status[1] and a shared
+// abort flag, after which no thread of the block waits again except the
+// producer for the copies it has already issued (the host reports
+// DNSLBM_ERR_TIMEOUT).
 #pragma once
 
 #include <cuda_fp16.h>
@@ -108,13 +110,26 @@ __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bu
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-constexpr int kWaitLimit = 1 << 22;  // try_wait rounds before a wait is declared lost
-
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ unsigned long long globaltimer_ns()
 {
-    for (int i = 0; i < kWaitLimit; ++i)
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `parity` of an mbarrier for at most limit_ns nanoseconds of
+// the GPU's global timer, or until another thread of the block has raised
+// the abort flag (none when abort is null).  Returns false when the wait
+// gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, unsigned long long limit_ns,
+                                                  volatile int *abort)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-    return false;
+        if ((abort && *abort) || globaltimer_ns() - t0 > limit_ns) return false;
+    }
 }
 
 // ------------------------------------------------------------------ rows
@@ -325,20 +340,187 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
     }
 }
 
+// ------------------------------------------------------------------ cell pairs
+// FP32 / FP16 storage: two neighbouring cells (x, x+1), x even, per thread
+// and iteration, collided together on the packed FP32 pipe (float2 values,
+// fma/add/mul .f32x2) -- half the arithmetic instructions per cell of the
+// one-cell form, with bit-identical populations (collide_lp.cuh).  A
+// direction whose source column is x itself (every direction of an even
+// step; e_x = 0 and the smooth-wall bounce-back of an odd step) moves both
+// cells' values with one 4-byte (FP16) or 8-byte (FP32) shared-memory
+// access; a direction shifted by e_x = +-1 in an odd step moves them one by
+// one.  For an odd nx the last pair has one cell: its second lane computes on
+// the row padding and is neither stored nor summed.  Textured wall planes use
+// the one-cell form (tma_group), whose wall links move per thread.
+template <typename T> struct PairIO;
+template <> struct PairIO<float> {
+    static __device__ __forceinline__ float2 ld2(const float *q) { return *reinterpret_cast<const float2 *>(q); }
+    static __device__ __forceinline__ void st2(float *q, float2 v) { *reinterpret_cast<float2 *>(q) = v; }
+    static __device__ __forceinline__ float ld1(const float *q) { return *q; }
+    static __device__ __forceinline__ void st1(float *q, float v) { *q = v; }
+};
+template <> struct PairIO<__half> {
+    static __device__ __forceinline__ float2 ld2(const __half *q)
+    {
+        return __half22float2(*reinterpret_cast<const __half2 *>(q));
+    }
+    static __device__ __forceinline__ void st2(__half *q, float2 v)
+    {
+        *reinterpret_cast<__half2 *>(q) = __floats2half2_rn(v.x, v.y);
+    }
+    static __device__ __forceinline__ float ld1(const __half *q) { return __half2float(*q); }
+    static __device__ __forceinline__ void st1(__half *q, float v) { *q = __float2half_rn(v); }
+};
+
+// WALL: 0 interior plane, -1 bottom plane, +1 top plane (smooth walls).
+template <typename T, bool ODD, bool CONSTQ, int WALL>
+__device__ __forceinline__ void tma_group2(const StepArgs &p, const LpParams &lk, T *sb, int dstride, int k,
+                                           const double *shift, double (&acc)[NP], int nc)
+{
+    using IO = PairIO<T>;
+    constexpr float iS = LpStore<T>::kInv;
+    const int nx = p.nx, pitch = p.pitch, npair = (nx + 1) >> 1;
+    const float2 c0 = vsplat<float2>((float)shift[0]), c1 = vsplat<float2>((float)shift[1]),
+                 c2 = vsplat<float2>((float)shift[2]);
+    float2 racc[NP];
+    float ncell = 0.f;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) racc[i] = make_float2(0.f, 0.f);
+    auto pair = [&](int j, int x) {
+        T *sbj = sb + (size_t)j * pitch;
+        const bool two = x + 1 < nx;
+        int xm0 = x, xp0 = x, xp1 = x;
+        if (ODD) {
+            xm0 = x == 0 ? nx - 1 : x - 1;
+            xp0 = x + 1 < nx ? x + 1 : 0;
+            xp1 = x + 2 < nx ? x + 2 : x + 2 - nx;
+        }
+        float2 f[Q];
+#pragma unroll
+        for (int A = 0; A < Q; ++A) {
+            const bool wdir = ODD && lat_ez(A) != 0 && lat_ez(A) == WALL;
+            const T *row = sbj + A * dstride;
+            float2 v;
+            if (!ODD || wdir || lat_ex(A) == 0) v = IO::ld2(row + x);
+            else if (lat_ex(A) > 0) v = make_float2(IO::ld1(row + xp0), IO::ld1(row + xp1));
+            else v = make_float2(IO::ld1(row + xm0), IO::ld1(row + x));
+            f[ODD ? lat_opp(A) : A] = v;
+        }
+        float2 s = make_float2(0.f, 0.f), m = make_float2(0.f, 0.f);
+        const LpCellV<float2> c = lp_collide_v<T, float2>(f, lk);
+        if (CONSTQ) {  // writer side: sums of the post-collision values
+            s = f[0];
+#pragma unroll
+            for (int a = 1; a < Q; ++a) s = vadd(s, f[a]);
+            bool first = true;
+#pragma unroll
+            for (int a = 0; a < Q; ++a) {
+                if (!lat_ex(a)) continue;
+                if (first) m = lat_ex(a) > 0 ? f[a] : vneg(f[a]);
+                else m = lat_ex(a) > 0 ? vadd(m, f[a]) : vsub(m, f[a]);
+                first = false;
+            }
+            s = vmul(s, vsplat<float2>(iS));
+            m = vmul(m, vsplat<float2>(iS));
+            if (WALL != 0) {  // smooth walls: every link into the wall bounces back, -2 e_x (w + d)
+                const int ap = WALL < 0 ? 12 : 11, am = WALL < 0 ? 13 : 14;
+                const float2 w36 = vsplat<float2>(1.f / 36.f), two_ = vsplat<float2>(2.f);
+                m = vsub(m, vmul(two_, vfma(f[ap], vsplat<float2>(iS), w36)));
+                m = vadd(m, vmul(two_, vfma(f[am], vsplat<float2>(iS), w36)));
+            }
+        }
+        const float2 d0 = vsub(c.u0, c0), d1 = vsub(c.u1, c1), d2 = vsub(c.u2, c2);
+        const float2 var = vfma(d2, d2, vfma(d1, d1, vmul(d0, d0)));
+        if (two) {
+            ncell += 2.f;
+            racc[0] = vadd(racc[0], c.drho);
+            racc[1] = vadd(racc[1], c.jx);
+            racc[2] = vadd(racc[2], c.u0);
+            racc[3] = vadd(racc[3], c.u1);
+            racc[4] = vadd(racc[4], c.u2);
+            racc[5] = vadd(racc[5], var);
+            if (CONSTQ) {
+                racc[6] = vadd(racc[6], s);
+                racc[7] = vadd(racc[7], m);
+            }
+        } else {
+            ncell += 1.f;
+            racc[0].x += c.drho.x;
+            racc[1].x += c.jx.x;
+            racc[2].x += c.u0.x;
+            racc[3].x += c.u1.x;
+            racc[4].x += c.u2.x;
+            racc[5].x += var.x;
+            if (CONSTQ) {
+                racc[6].x += s.x;
+                racc[7].x += m.x;
+            }
+        }
+#pragma unroll
+        for (int A = 0; A < Q; ++A) {
+            const bool wdir = ODD && lat_ez(A) != 0 && lat_ez(A) == WALL;
+            T *row = sbj + A * dstride;
+            const float2 v = f[ODD ? A : lat_opp(A)];
+            if (!ODD || wdir || lat_ex(A) == 0) {
+                IO::st2(row + x, v);  // for a one-cell pair the second lane lands in the row padding
+            } else if (lat_ex(A) > 0) {
+                IO::st1(row + xp0, v.x);
+                if (two) IO::st1(row + xp1, v.y);
+            } else {
+                IO::st1(row + xm0, v.x);
+                if (two) IO::st1(row + x, v.y);
+            }
+        }
+    };
+    // the FP32 partial sums of a row go to the FP64 accumulators when the
+    // thread moves to another row; slots 0 and 6 sum 1 + deviation per cell
+    auto flush = [&]() {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            if (i >= 6 && !CONSTQ) continue;
+            if (i == 0 || i == 6) acc[i] += (double)ncell;
+            acc[i] += (double)racc[i].x + (double)racc[i].y;
+            racc[i] = make_float2(0.f, 0.f);
+        }
+        ncell = 0.f;
+    };
+    // the group's k * npair pairs as one range over the consumer threads
+    int j = 0, pr = threadIdx.x, jr = 0;
+    while (pr >= npair && j < k) pr -= npair, ++j;
+    jr = j;
+    for (; j < k; pr += nc) {
+        while (pr >= npair) pr -= npair, ++j;
+        if (j >= k) break;
+        if (j != jr) flush(), jr = j;
+        pair(j, 2 * pr);
+    }
+    flush();
+}
+
 // ------------------------------------------------------------------ kernel
 // Producer warp: lane A < 19 moves direction A's rows of every row group of
 // the block; lane 0 also arms the stage's full barrier with the byte count.
+// When a wait of the block gives up (the abort flag), the producer issues no
+// further copy and, before it returns, waits for every load it has issued
+// and every store it has committed, so no bulk copy into or out of the
+// block's shared memory outlives the block.
+// p.withhold_stage (a test switch, 0 in every normal launch) makes block 0
+// neither arm nor load its first row group: its consumers' first wait then
+// runs out after p.wait_ns with no copy in flight on that stage.
 template <typename T, bool ODD, int TEX>
 __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t, int g0, int n, int lane,
                                              unsigned char *smem, uint64_t *full, uint64_t *empty, volatile int *abort)
 {
     const int S = t.stages;
     const size_t dir_bytes = (size_t)t.k * t.row_bytes, stage_bytes = (size_t)Q * dir_bytes;
+    const bool withhold = p.withhold_stage != 0 && g0 == 0;
+    unsigned loaded = 0;  // bit s: a load into stage s was issued (its phase is the last one armed)
+    unsigned phase = 0;   // bit s: parity of that phase
     for (int i = 0; i < n + S; ++i) {
         const int st = i % S;
         unsigned char *stage = smem + (size_t)st * stage_bytes;
         if (i >= S) {  // store group i - S once the consumers have released its stage
-            if (!*abort && !mbar_wait_bounded(empty + st, (uint32_t)((i / S - 1) & 1))) {
+            if (!*abort && !mbar_wait_bounded(empty + st, (uint32_t)((i / S - 1) & 1), p.wait_ns, abort)) {
                 *abort = 1;
                 atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
             }
@@ -364,13 +546,24 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && g.bulk);
             if (lane < Q) bulk_wait_read_all();  // this lane's store of the stage has read it
             __syncwarp();
-            if (lane == 0) mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * t.row_bytes));
-            __syncwarp();
-            if (lane < Q && g.bulk && !*abort)
-                copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, true, full + st);
+            // one decision for the whole warp: lane 0's reading of the flag
+            const bool issue = __shfl_sync(0xffffffffu, *abort, 0) == 0 && !(withhold && i == 0);
+            if (issue) {
+                if (lane == 0) mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * t.row_bytes));
+                __syncwarp();
+                if (lane < Q && g.bulk) copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, true, full + st);
+                loaded |= 1u << st;
+                phase = (phase & ~(1u << st)) | ((unsigned)((i / S) & 1) << st);
+            }
         }
     }
     if (lane < Q) bulk_wait_all();
+    if (*abort) {
+        // loads still landing in shared memory: wait for the last phase armed
+        // on each stage (bounded; a load that was issued does complete)
+        for (int st = 0; st < S; ++st)
+            if ((loaded >> st) & 1u) mbar_wait_bounded(full + st, (phase >> st) & 1u, p.wait_ns, nullptr);
+    }
 }
 
 constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer warp
@@ -407,6 +600,8 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
     const double G = CONSTQ ? p.force[step & 1] : p.gx;
     const double *shift_now = p.shift + (size_t)(step & 1) * p.nz * 3;
     const int dstride = t.k * p.pitch;
+    [[maybe_unused]] const LpParams lk = lp_params<typename std::conditional<std::is_same<T, double>::value, float, T>::type>(
+        (float)p.omega, (float)G);
     double acc[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) acc[i] = 0.0;
@@ -415,16 +610,29 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
         int z, y0;
         group_origin(t, gi, z, y0);
         const int k = min(t.k, p.ny - y0);
-        if (!*(volatile int *)&s_abort && !mbar_wait_bounded(full + st, (uint32_t)((i / S) & 1))) {
+        if (!*(volatile int *)&s_abort &&
+            !mbar_wait_bounded(full + st, (uint32_t)((i / S) & 1), p.wait_ns, (volatile int *)&s_abort)) {
             s_abort = 1;
             atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
         }
         T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
         const double *sh = shift_now + z * 3;
         constexpr bool TXT = TEX != 0;
-        if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-        else if (z == p.nz - 1) tma_group<T, ODD, CONSTQ, TXT, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-        else tma_group<T, ODD, CONSTQ, TXT, 0>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        if constexpr (std::is_same<T, double>::value) {
+            if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+            else if (z == p.nz - 1) tma_group<T, ODD, CONSTQ, TXT, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+            else tma_group<T, ODD, CONSTQ, TXT, 0>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        } else {
+            if (z == 0) {
+                if (TXT) tma_group<T, ODD, CONSTQ, true, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+                else tma_group2<T, ODD, CONSTQ, -1>(p, lk, sb, dstride, k, sh, acc, nc);
+            } else if (z == p.nz - 1) {
+                if (TXT) tma_group<T, ODD, CONSTQ, true, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+                else tma_group2<T, ODD, CONSTQ, 1>(p, lk, sb, dstride, k, sh, acc, nc);
+            } else {
+                tma_group2<T, ODD, CONSTQ, 0>(p, lk, sb, dstride, k, sh, acc, nc);
+            }
+        }
         fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);

@@ -78,6 +78,8 @@ def lib():
     L.dnslbm_moments.argtypes = [vp, dp, dp]
     L.dnslbm_step_timed.argtypes = [vp, ctypes.c_long, dp, dp, dp]
     L.dnslbm_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    L.dnslbm_set_wait_limit.argtypes = [vp, ctypes.c_double]
+    L.dnslbm_test_withhold_load.argtypes = [vp]
     L.dnslbm_step_kernel.argtypes = [vp]
     L.dnslbm_step_kernel.restype = ctypes.c_char_p
     L.dnslbm_bytes_per_cell.argtypes = [vp]
@@ -190,6 +192,15 @@ class Channel:
         t, e, o = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         self._ck(self.L.dnslbm_step_timed(self.h, n, ctypes.byref(t), ctypes.byref(e), ctypes.byref(o)))
         return t.value, e.value, o.value
+
+    def set_wait_limit(self, ms):
+        """Limit (ms) of the row-pipelined kernel's bounded device waits."""
+        self._ck(self.L.dnslbm_set_wait_limit(self.h, ms))
+
+    def test_withhold_load(self):
+        """Test hook: the next bulk-copy launch withholds one load, so a
+        bounded wait runs out and that step call raises ERR_TIMEOUT."""
+        self._ck(self.L.dnslbm_test_withhold_load(self.h))
 
     @property
     def steps_done(self):

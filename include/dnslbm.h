@@ -177,6 +177,23 @@ int dnslbm_step_timed(dnslbm_ctx *ctx, long nsteps, double *ms_total, double *ms
  * (definitions.h:117). */
 int dnslbm_autotune(dnslbm_ctx *ctx, int steps, char *report, size_t report_len);
 
+/* Limit of each bounded device-side wait of the row-pipelined step kernel
+ * (its consumers waiting for a bulk copy to land, its producer waiting for
+ * them to release a stage), in milliseconds of the GPU's global timer;
+ * default 1000.  A wait that runs out ends that block's part of the step
+ * early (no copy left in flight) and the step call returns
+ * DNSLBM_ERR_TIMEOUT; the state is then invalid until the next load.  No
+ * counterpart in the reference, whose MPI waits are unbounded
+ * (xcomputations.c:435-555). */
+int dnslbm_set_wait_limit(dnslbm_ctx *ctx, double ms);
+/* Test hook for the bounded waits (no counterpart in the reference): the
+ * next launch of the row-pipelined kernel has its first block withhold the
+ * load of its first row group, so that block's consumers wait for data that
+ * never comes, give up after the wait limit, and the step call returns
+ * DNSLBM_ERR_TIMEOUT.  Nothing faults and no copy is left in flight.
+ * DNSLBM_ERR_STATE when the context steps with the per-thread kernel. */
+int dnslbm_test_withhold_load(dnslbm_ctx *ctx);
+
 /* Name of the step kernel this context launches ("row-pipelined bulk-copy"
  * or "per-thread"), with its launch shape. */
 const char *dnslbm_step_kernel(const dnslbm_ctx *ctx);

@@ -47,7 +47,7 @@ def collide_f32(r, omega, g, unbiased):
     else:
         inv = f32(1) / rho
         u = [jj * inv for jj in j]
-    usq15 = f32(1.5) * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2])
+    usq15 = f32(1.5) * fma(u[2], u[2], fma(u[1], u[1], u[0] * u[0]))
     om1 = f32(1) - om
     out = [None] * 19
     out[0] = fma(om1, r[0], f32(1 / 3) * fma(om, fma(rho, -usq15, dr), f32(-3) * G * u[0]))
