@@ -24,6 +24,7 @@ void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int row
                   double *partials, double *plane_out, cudaStream_t s);
 void launch_stats_sample(int nz, double np, const double *planes, double *mean, double *acc, bool accumulate,
                          cudaStream_t s);
+void launch_stats_rows(int nz, double np, const double *mean, const double *planes, double *out, cudaStream_t s);
 int tma_prepare_f64(size_t smem);
 int tma_occupancy_f64(int threads, size_t smem);
 void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
@@ -76,6 +77,13 @@ struct dnslbm_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;                // the per-cell pass runs here beside the bulk kernel
     cudaEvent_t fj[2] = {nullptr, nullptr};     // fork / join of the side stream
+    // asynchronous output (dnslbm_output_begin): device buffers of one
+    // snapshot, the stream their copies to the host run on, and the events
+    // that order them (ready: kernels done; done: copies landed)
+    double *out_lbf = nullptr, *out_vel = nullptr, *out_den = nullptr, *out_stats = nullptr;
+    cudaStream_t out_stream = nullptr;
+    cudaEvent_t out_ev[2] = {nullptr, nullptr};
+    int out_pending = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> tev;  // per-launch timing events
     dim3 grid, block;
@@ -166,7 +174,8 @@ static void free_all(dnslbm_ctx *c)
     void *ptrs[] = {c->popmem,     c->wallmask,   c->force,         c->shift,       c->partials,
                     c->plane_sums, c->logs,       c->step_ctr,      c->status,      c->plane_ctr,
                     c->total_ctr,  c->staging,    c->stat_partials, c->stat_planes, c->stat_mean,
-                    c->band_of,    c->links,      c->plane_list,    c->d_llaunch,   c->stat_acc};
+                    c->band_of,    c->links,      c->plane_list,    c->d_llaunch,   c->stat_acc,
+                    c->out_lbf,    c->out_vel,    c->out_den,       c->out_stats};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : c->ev)
@@ -175,6 +184,9 @@ static void free_all(dnslbm_ctx *c)
         if (e) cudaEventDestroy(e);
     for (auto &e : c->fj)
         if (e) cudaEventDestroy(e);
+    for (auto &e : c->out_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->out_stream) cudaStreamDestroy(c->out_stream);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -385,6 +397,9 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     }
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->out_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->out_ev[1], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->fj[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->fj[1], cudaEventDisableTiming) != cudaSuccess) {
         fail(c, DNSLBM_ERR_CUDA, "cannot create streams");
@@ -1002,6 +1017,77 @@ extern "C" int dnslbm_statistics(dnslbm_ctx *c, double *out)
         REYS[z + 1] = pl[z * 5 + 3] / np;
         DTIN[z + 1] = std::sqrt(pl[z * 5 + 4] / np);
     }
+    return DNSLBM_OK;
+}
+
+// ---------------------------------------------------------------- output
+// dnslbm_output_begin: the outputs of the current state are computed on the
+// context's stream (so later steps see the state only after the kernels
+// that read it) into device buffers, and copied to the caller's host
+// buffers on out_stream while the steps that follow run.
+static int out_alloc(dnslbm_ctx *c, double **p, size_t n)
+{
+    if (*p) return DNSLBM_OK;
+    cudaError_t e = cudaMalloc(p, n * sizeof(double));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(c, DNSLBM_ERR_NOMEM, "cudaMalloc of %zu bytes for an output snapshot failed: %s",
+                    n * sizeof(double), cudaGetErrorString(e));
+    }
+    CK(cudaMemset(*p, 0, n * sizeof(double)));  // wall-plane entries stay zero
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_output_begin(dnslbm_ctx *c, double *state, double *vel, double *den, double *stats)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    CK(cudaSetDevice(c->deck.device));
+    const size_t cells = (size_t)c->nx * c->ny * (c->nz + 2);
+    const int zd = c->nz + 2;
+    int rc;
+    if (state && (rc = out_alloc(c, &c->out_lbf, cells * Q))) return rc;
+    if ((vel || den) && ((rc = out_alloc(c, &c->out_vel, cells * 3)) || (rc = out_alloc(c, &c->out_den, cells))))
+        return rc;
+    if (stats && (rc = out_alloc(c, &c->out_stats, (size_t)9 * zd))) return rc;
+    CK(cudaDeviceSynchronize());  // the allocations' zero fill
+    // the previous snapshot's copies read these buffers: wait on the device
+    if (c->out_pending) CK(cudaStreamWaitEvent(c->stream, c->out_ev[1], 0));
+    IoArgs p = io_args(c);
+    if (state) launch_io(c->deck.precision, 0, p, 0, c->nx, c->out_lbf, nullptr, c->stream);
+    if (vel || den) launch_io(c->deck.precision, 3, p, 0, c->nx, c->out_vel, c->out_den, c->stream);
+    if (stats) {
+        const double np = (double)c->nx * c->ny;
+        launch_stats(c->deck.precision, p, c->grid, c->block, c->rows, 0, nullptr, c->stat_partials, c->stat_planes,
+                     c->stream);
+        launch_stats_sample(c->nz, np, c->stat_planes, c->stat_mean, nullptr, false, c->stream);
+        launch_stats(c->deck.precision, p, c->grid, c->block, c->rows, 1, c->stat_mean, c->stat_partials,
+                     c->stat_planes, c->stream);
+        launch_stats_rows(c->nz, np, c->stat_mean, c->stat_planes, c->out_stats, c->stream);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->out_ev[0], c->stream));
+    CK(cudaStreamWaitEvent(c->out_stream, c->out_ev[0], 0));
+    if (state)
+        CK(cudaMemcpyAsync(state, c->out_lbf, cells * Q * sizeof(double), cudaMemcpyDeviceToHost, c->out_stream));
+    if (vel) CK(cudaMemcpyAsync(vel, c->out_vel, cells * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->out_stream));
+    if (den) CK(cudaMemcpyAsync(den, c->out_den, cells * sizeof(double), cudaMemcpyDeviceToHost, c->out_stream));
+    if (stats)
+        CK(cudaMemcpyAsync(stats, c->out_stats, (size_t)9 * zd * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->out_stream));
+    CK(cudaEventRecord(c->out_ev[1], c->out_stream));
+    c->out_pending = 1;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_output_wait(dnslbm_ctx *c)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->out_pending) return DNSLBM_OK;
+    CK(cudaSetDevice(c->deck.device));
+    CK(cudaEventSynchronize(c->out_ev[1]));
+    c->out_pending = 0;
     return DNSLBM_OK;
 }
 

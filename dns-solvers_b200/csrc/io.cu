@@ -301,6 +301,26 @@ __global__ void stats_accumulate_kernel(const double *planes, const double *mean
     acc[8 * nz + z] += pl[4] / np;
 }
 
+// The statistics rows of one sample in the turb-fld layout [9][nz + 2]
+// (statistics.c:139-147 file order; wall entries left as they are): plane
+// means from pass 0 (mean[z][u v w rho]) and the pass-1 second-moment sums.
+__global__ void stats_rows_kernel(const double *mean, const double *planes, int nz, double np, double *out)
+{
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nz) return;
+    const int zd = nz + 2;
+    const double *pl = planes + (size_t)z * NS;
+    out[0 * zd + z + 1] = mean[z * 4 + 0];
+    out[1 * zd + z + 1] = mean[z * 4 + 1];
+    out[2 * zd + z + 1] = mean[z * 4 + 2];
+    out[3 * zd + z + 1] = sqrt(pl[0] / np);
+    out[4 * zd + z + 1] = sqrt(pl[1] / np);
+    out[5 * zd + z + 1] = sqrt(pl[2] / np);
+    out[6 * zd + z + 1] = pl[3] / np;
+    out[7 * zd + z + 1] = mean[z * 4 + 3];
+    out[8 * zd + z + 1] = sqrt(pl[4] / np);
+}
+
 // ---------------------------------------------------------------- launchers
 template <typename T>
 static void io_dispatch(int what, const IoArgs &p, int x0, int nxc, double *a, double *b, cudaStream_t s)
@@ -335,6 +355,12 @@ void launch_stats_sample(int nz, double np, const double *planes, double *mean, 
     const int bs = 128, nb = (nz + bs - 1) / bs;
     if (accumulate) stats_accumulate_kernel<<<nb, bs, 0, s>>>(planes, mean, nz, np, acc);
     else stats_means_kernel<<<nb, bs, 0, s>>>(planes, nz, np, mean);
+}
+
+void launch_stats_rows(int nz, double np, const double *mean, const double *planes, double *out, cudaStream_t s)
+{
+    const int bs = 128;
+    stats_rows_kernel<<<(nz + bs - 1) / bs, bs, 0, s>>>(mean, planes, nz, np, out);
 }
 
 void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int rows, int pass, const double *mean,

@@ -29,6 +29,15 @@ __device__ __forceinline__ RegT<T> ld_raw(const T *q)
     if constexpr (std::is_same<T, double>::value) return *q;
     else return LpStore<T>::ld(q);
 }
+// Global-memory load that bypasses L1 (ld.global.cg): a population that
+// another SM wrote earlier in the same launch (the persistent batch kernel
+// runs many steps in one launch) is read from L2, never from a stale L1 line.
+template <typename T>
+__device__ __forceinline__ RegT<T> ld_glb(const T *q)
+{
+    if constexpr (std::is_same<T, __half>::value) return __half2float(__ldcg(q));
+    else return __ldcg(q);
+}
 template <typename T>
 __device__ __forceinline__ void st_raw(T *q, RegT<T> v)
 {
@@ -137,7 +146,7 @@ __device__ __forceinline__ void links_cell(const StepArgs &p, const Nbr &n, int 
         V f[Q];
 #pragma unroll
         for (int A = 0; A < Q; ++A)
-            f[A] = (!ODD && sbx) ? ld_raw<T>(sbx + A * dstride) : ld_raw<T>(static_cast<const T *>(p.pop[A]) + n.c0);
+            f[A] = (!ODD && sbx) ? ld_raw<T>(sbx + A * dstride) : ld_glb<T>(static_cast<const T *>(p.pop[A]) + n.c0);
         solid_sums<T, CONSTQ>(f, c0, c1, c2, acc, racc);
         return;
     }
@@ -146,8 +155,8 @@ __device__ __forceinline__ void links_cell(const StepArgs &p, const Nbr &n, int 
         constexpr int A = decltype(ac)::value;
         V v;
         if (!ODD && sbx) v = ld_raw<T>(sbx + A * dstride);
-        else if (!ODD) v = ld_raw<T>(static_cast<const T *>(p.pop[A]) + n.c0);
-        else v = ld_raw<T>(links_ptr<T, A>(p, n, wall, lk));
+        else if (!ODD) v = ld_glb<T>(static_cast<const T *>(p.pop[A]) + n.c0);
+        else v = ld_glb<T>(links_ptr<T, A>(p, n, wall, lk));
         f[ODD ? lat_opp(A) : A] = v;
     });
     if constexpr (std::is_same<T, double>::value) {

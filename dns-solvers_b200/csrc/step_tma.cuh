@@ -230,7 +230,7 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
                     AD(10) AD(11) AD(12) AD(13) AD(14) AD(15) AD(16) AD(17) AD(18)
 #undef AD
                 }
-                v = ld_raw<T>(static_cast<const T *>(p.pop[slot]) + idx);
+                v = ld_glb<T>(static_cast<const T *>(p.pop[slot]) + idx);
             } else {
                 const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
                 v = ld_raw<T>(sbj + A * dstride + xs);

@@ -78,6 +78,8 @@ def lib():
     L.dnslbm_moments.argtypes = [vp, dp, dp]
     L.dnslbm_step_timed.argtypes = [vp, ctypes.c_long, dp, dp, dp]
     L.dnslbm_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    L.dnslbm_output_begin.argtypes = [vp, dp, dp, dp, dp]
+    L.dnslbm_output_wait.argtypes = [vp]
     L.dnslbm_set_wait_limit.argtypes = [vp, ctypes.c_double]
     L.dnslbm_test_withhold_load.argtypes = [vp]
     L.dnslbm_step_kernel.argtypes = [vp]
@@ -193,6 +195,24 @@ class Channel:
         self._ck(self.L.dnslbm_step_timed(self.h, n, ctypes.byref(t), ctypes.byref(e), ctypes.byref(o)))
         return t.value, e.value, o.value
 
+    def output_begin(self, state=None, vel=None, den=None, stats=None):
+        """Start the asynchronous output of the current state into the given
+        host arrays (page-locked for overlap: PinnedArray); they are valid
+        after output_wait()."""
+        shapes = {"state": self.state_shape, "vel": self.state_shape[:3] + (3,), "den": self.state_shape[:3],
+                  "stats": (9, self.shape[2] + 2)}
+        ptrs = []
+        for name, a in (("state", state), ("vel", vel), ("den", den), ("stats", stats)):
+            if a is None:
+                ptrs.append(None)
+                continue
+            assert a.shape == shapes[name] and a.dtype == np.float64 and a.flags.c_contiguous, name
+            ptrs.append(_dp(a))
+        self._ck(self.L.dnslbm_output_begin(self.h, *ptrs))
+
+    def output_wait(self):
+        self._ck(self.L.dnslbm_output_wait(self.h))
+
     def set_wait_limit(self, ms):
         """Limit (ms) of the row-pipelined kernel's bounded device waits."""
         self._ck(self.L.dnslbm_set_wait_limit(self.h, ms))
@@ -237,10 +257,13 @@ class Channel:
 
     def stats_reset(self):
         self._ck(self.L.dnslbm_stats_reset(self.h))
-    def moments(self):
+    def moments(self, vel=None, den=None):
         x, y, z = self.shape
-        vel = np.zeros((x, y, z + 2, 3))
-        den = np.zeros((x, y, z + 2))
+        if vel is None:
+            vel = np.zeros((x, y, z + 2, 3))
+        if den is None:
+            den = np.zeros((x, y, z + 2))
+        assert vel.shape == (x, y, z + 2, 3) and den.shape == (x, y, z + 2)
         self._ck(self.L.dnslbm_moments(self.h, _dp(vel), _dp(den)))
         return vel, den
 

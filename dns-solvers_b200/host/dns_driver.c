@@ -19,6 +19,11 @@
  *   RIBH RIBS (riblet height and spacing; riblets select the general wall
  *   rule, DNSLBM_BC_GENERAL)
  *   PRECISION 64|32|16   FORCE q|g   GX   DEVICE   OMEGA (overrides Rebs)
+ *   ASYNC 1|0   output without stopping the time loop (default 1): at an
+ *               output step the library computes the outputs on the GPU and
+ *               copies them to page-locked host buffers while the next steps
+ *               run (dnslbm_output_begin), and a writer thread writes the
+ *               files; 0 stores, writes and only then steps on
  *
  * Files written (formats of the reference):
  *   energy.txt flowrate.txt massrate.txt   encalc.c:125-138, every step
@@ -31,6 +36,7 @@
  * step overwrites before reading) holds the state again.
  */
 #include <errno.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -42,7 +48,7 @@
 typedef struct {
     double Rebs, ub, CFL, GX, OMEGA;
     int zdv, ydv, xdv, TSTR, TEND, ITER, RSLIP, PSLIP;
-    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS;
+    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS, ASYNC;
     char TEXTURE[32], FORCE[8];
 } Deck;
 
@@ -68,6 +74,7 @@ static void deck_defaults(Deck *d)
     d->PWY = 2;
     d->RIBH = 8;
     d->RIBS = 16;
+    d->ASYNC = 1;
     strcpy(d->TEXTURE, "smooth");
     strcpy(d->FORCE, "q");
 }
@@ -79,7 +86,7 @@ static int deck_set(Deck *d, const char *k, const char *v)
 #define STR(N) if (!strcmp(k, #N)) { snprintf(d->N, sizeof d->N, "%s", v); return 0; }
     DBL(Rebs) DBL(ub) DBL(CFL) DBL(GX) DBL(OMEGA)
     INT(zdv) INT(ydv) INT(xdv) INT(TSTR) INT(TEND) INT(ITER) INT(RSLIP) INT(PSLIP)
-    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS)
+    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS) INT(ASYNC)
     STR(TEXTURE) STR(FORCE)
 #undef DBL
 #undef INT
@@ -131,6 +138,108 @@ static int write_file(const char *fn, const void *p, size_t bytes, size_t copies
             return -1;
         }
     return fclose(f);
+}
+
+/* One output event's files: lbf/force (checkpoints only), vel, den,
+ * turb-fld and uavg-temp.dat, from host buffers. */
+typedef struct {
+    double *state, *vel, *den, *stats;
+    double force;
+    long label;
+    int checkpoint;
+} Snapshot;
+
+typedef struct {
+    size_t state_n, ncol;
+    int zd;
+} Shape;
+
+static int write_snapshot(const Snapshot *sn, const Shape *sh)
+{
+    char fn[64];
+    if (sn->checkpoint) {
+        snprintf(fn, sizeof fn, "lbf.%.4ld", sn->label);
+        if (write_file(fn, sn->state, sh->state_n * sizeof(double), 2)) return -1;
+        snprintf(fn, sizeof fn, "force.%.4ld", sn->label);
+        if (write_file(fn, &sn->force, sizeof sn->force, 1)) return -1;
+    }
+    snprintf(fn, sizeof fn, "vel.%.4d", (int)sn->label);
+    if (write_file(fn, sn->vel, sh->ncol * sh->zd * 3 * sizeof(double), 1)) return -1;
+    snprintf(fn, sizeof fn, "den.%.4d", (int)sn->label);
+    if (write_file(fn, sn->den, sh->ncol * sh->zd * sizeof(double), 1)) return -1;
+    snprintf(fn, sizeof fn, "turb-fld.%.3d.%.3ld", 0, sn->label);
+    if (write_file(fn, sn->stats, 9 * sh->zd * sizeof(double), 1)) return -1;
+    FILE *u = fopen("uavg-temp.dat", "w");
+    if (u) {
+        const int zd = sh->zd;
+        for (int k = 0; k < zd; k++) {
+            double z = k == 0 ? 0. : (k == zd - 1 ? zd - 2. : k - 0.5);
+            fprintf(u, "%.12f %.12f\n", z / (zd - 2.), sn->stats[k]);
+        }
+        fclose(u);
+    }
+    return 0;
+}
+
+/* The writer thread: one job at a time, handed over by the time loop. */
+typedef struct {
+    pthread_t th;
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
+    const Snapshot *job;  /* pending job, NULL when idle */
+    const Shape *shape;
+    int quit, failed;
+} Writer;
+
+static void *writer_main(void *arg)
+{
+    Writer *w = arg;
+    pthread_mutex_lock(&w->mu);
+    for (;;) {
+        while (!w->job && !w->quit) pthread_cond_wait(&w->cv, &w->mu);
+        if (!w->job) break;
+        const Snapshot *sn = w->job;
+        pthread_mutex_unlock(&w->mu);
+        const int bad = write_snapshot(sn, w->shape);
+        pthread_mutex_lock(&w->mu);
+        if (bad) w->failed = 1;
+        w->job = NULL;
+        pthread_cond_broadcast(&w->cv);
+    }
+    pthread_mutex_unlock(&w->mu);
+    return NULL;
+}
+
+/* Wait until the writer is idle; returns nonzero if a write failed. */
+static int writer_wait(Writer *w)
+{
+    pthread_mutex_lock(&w->mu);
+    while (w->job) pthread_cond_wait(&w->cv, &w->mu);
+    const int failed = w->failed;
+    pthread_mutex_unlock(&w->mu);
+    return failed;
+}
+
+static void writer_submit(Writer *w, const Snapshot *sn)
+{
+    pthread_mutex_lock(&w->mu);
+    w->job = sn;
+    pthread_cond_broadcast(&w->cv);
+    pthread_mutex_unlock(&w->mu);
+}
+
+/* Page-locked when possible (the copies then overlap the steps). */
+static double *host_buffer(size_t n, int *pinned)
+{
+    double *p = dnslbm_host_alloc(n * sizeof(double));
+    *pinned = p != NULL;
+    return p ? p : malloc(n * sizeof(double));
+}
+
+static void host_buffer_free(double *p, int pinned)
+{
+    if (pinned) dnslbm_host_free(p);
+    else free(p);
 }
 
 int main(int argc, char **argv)
@@ -228,47 +337,64 @@ int main(int argc, char **argv)
         fprintf(stderr, "END OF READING DATA FROM FILES\nSTARTING FROM %d\n", TM);
     }
 
-    double *vel = malloc(ncol * zd * 3 * sizeof(double)), *den = malloc(ncol * zd * sizeof(double));
-    double *stats = malloc(9 * zd * sizeof(double));
+    /* Output buffers: one checkpoint state (checkpoints are ten output
+     * events apart, so the writer is long done with it) and two sets of
+     * vel/den/turb-fld, one being filled while the writer drains the other.
+     * The synchronous mode uses the first set and the state array. */
+    const Shape shape = {state_n, ncol, zd};
+    Snapshot snap[2];
+    int pin_state = 0, pin[2][3] = {{0}};
+    double *ckpt = D.ASYNC ? host_buffer(state_n, &pin_state) : state;
+    for (int i = 0; i < 2; i++) {
+        snap[i].state = ckpt;
+        snap[i].vel = host_buffer(ncol * zd * 3, &pin[i][0]);
+        snap[i].den = host_buffer(ncol * zd, &pin[i][1]);
+        snap[i].stats = host_buffer(9 * (size_t)zd, &pin[i][2]);
+    }
     const long cap = 4096;
     double *logs = malloc(cap * DNSLBM_LOG_N * sizeof(double));
-    if (!vel || !den || !stats || !logs) {
+    int bad_alloc = !ckpt || !logs;
+    for (int i = 0; i < 2; i++) bad_alloc |= !snap[i].vel || !snap[i].den || !snap[i].stats;
+    if (bad_alloc) {
         fprintf(stderr, "run-dns: host allocation failed\n");
+        return 1;
+    }
+    Writer W = {.job = NULL, .shape = &shape, .quit = 0, .failed = 0};
+    pthread_mutex_init(&W.mu, NULL);
+    pthread_cond_init(&W.cv, NULL);
+    if (D.ASYNC && pthread_create(&W.th, NULL, writer_main, &W)) {
+        fprintf(stderr, "run-dns: cannot start the writer thread\n");
         return 1;
     }
 
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
-    long ss = 0;
+    long ss = 0, nout = 0;
     int nan_stop = 0;
     while (ss < up + 1 && !nan_stop) {
         if (!(ss % utime)) {
-            const long label = TM + ss / utime;
-            if (!(ss % (10 * utime))) {
-                if ((rc = dnslbm_store_state(c, state))) return die(c, rc, "dnslbm_store_state");
-                snprintf(fn, sizeof fn, "lbf.%.4ld", label);
-                if (write_file(fn, state, state_n * sizeof(double), 2)) return die(c, DNSLBM_ERR_IO, fn);
-                double force;
-                if ((rc = dnslbm_get_force(c, &force))) return die(c, rc, "dnslbm_get_force");
-                snprintf(fn, sizeof fn, "force.%.4ld", label);
-                if (write_file(fn, &force, sizeof force, 1)) return die(c, DNSLBM_ERR_IO, fn);
-            }
-            if ((rc = dnslbm_moments(c, vel, den))) return die(c, rc, "dnslbm_moments");
-            snprintf(fn, sizeof fn, "vel.%.4d", (int)label);
-            if (write_file(fn, vel, ncol * zd * 3 * sizeof(double), 1)) return die(c, DNSLBM_ERR_IO, fn);
-            snprintf(fn, sizeof fn, "den.%.4d", (int)label);
-            if (write_file(fn, den, ncol * zd * sizeof(double), 1)) return die(c, DNSLBM_ERR_IO, fn);
-            if ((rc = dnslbm_statistics(c, stats))) return die(c, rc, "dnslbm_statistics");
-            snprintf(fn, sizeof fn, "turb-fld.%.3d.%.3ld", 0, label);
-            if (write_file(fn, stats, 9 * zd * sizeof(double), 1)) return die(c, DNSLBM_ERR_IO, fn);
-            FILE *u = fopen("uavg-temp.dat", "w");
-            if (u) {
-                for (int k = 0; k < zd; k++) {
-                    double z = k == 0 ? 0. : (k == zd - 1 ? zd - 2. : k - 0.5);
-                    fprintf(u, "%.12f %.12f\n", z / (zd - 2.), stats[k]);
+            Snapshot *sn = &snap[nout & 1];
+            sn->label = TM + ss / utime;
+            sn->checkpoint = !(ss % (10 * utime));
+            if (sn->checkpoint && (rc = dnslbm_get_force(c, &sn->force))) return die(c, rc, "dnslbm_get_force");
+            if (D.ASYNC) {
+                /* the previous event's copies have landed (the steps since
+                 * took longer); hand them to the writer once it is done with
+                 * the event before, whose buffers this event reuses */
+                if (nout > 0) {
+                    if ((rc = dnslbm_output_wait(c))) return die(c, rc, "dnslbm_output_wait");
+                    if (writer_wait(&W)) return die(c, DNSLBM_ERR_IO, "writing an output file");
+                    writer_submit(&W, &snap[(nout - 1) & 1]);
                 }
-                fclose(u);
+                if ((rc = dnslbm_output_begin(c, sn->checkpoint ? sn->state : NULL, sn->vel, sn->den, sn->stats)))
+                    return die(c, rc, "dnslbm_output_begin");
+            } else {
+                if (sn->checkpoint && (rc = dnslbm_store_state(c, sn->state))) return die(c, rc, "dnslbm_store_state");
+                if ((rc = dnslbm_moments(c, sn->vel, sn->den))) return die(c, rc, "dnslbm_moments");
+                if ((rc = dnslbm_statistics(c, sn->stats))) return die(c, rc, "dnslbm_statistics");
+                if (write_snapshot(sn, &shape)) return die(c, DNSLBM_ERR_IO, "writing an output file");
             }
+            nout++;
         }
         /* steps up to the next output event, in one device batch */
         long n = utime - ss % utime;
@@ -316,6 +442,20 @@ int main(int argc, char **argv)
         }
         ss += n;
     }
+    if (D.ASYNC) {
+        if (nout > 0) {
+            if ((rc = dnslbm_output_wait(c))) return die(c, rc, "dnslbm_output_wait");
+            if (writer_wait(&W)) return die(c, DNSLBM_ERR_IO, "writing an output file");
+            writer_submit(&W, &snap[(nout - 1) & 1]);
+        }
+        const int failed = writer_wait(&W);
+        pthread_mutex_lock(&W.mu);
+        W.quit = 1;
+        pthread_cond_broadcast(&W.cv);
+        pthread_mutex_unlock(&W.mu);
+        pthread_join(W.th, NULL);
+        if (failed) return die(c, DNSLBM_ERR_IO, "writing an output file");
+    }
     clock_gettime(CLOCK_MONOTONIC, &t1);
     const double secs = (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
 
@@ -335,10 +475,15 @@ int main(int argc, char **argv)
     }
     free(flags);
     free(state);
-    free(vel);
-    free(den);
-    free(stats);
+    if (D.ASYNC) host_buffer_free(ckpt, pin_state);
+    for (int i = 0; i < 2; i++) {
+        host_buffer_free(snap[i].vel, pin[i][0]);
+        host_buffer_free(snap[i].den, pin[i][1]);
+        host_buffer_free(snap[i].stats, pin[i][2]);
+    }
     free(logs);
+    pthread_mutex_destroy(&W.mu);
+    pthread_cond_destroy(&W.cv);
     dnslbm_destroy(c);
     return nan_stop ? 1 : 0;
 }

@@ -163,6 +163,23 @@ int dnslbm_stats_reset(dnslbm_ctx *ctx);
 /* vel_print.c:65-99 of the current state (either pointer may be NULL). */
 int dnslbm_moments(dnslbm_ctx *ctx, double *vel, double *den);
 
+/* Output without stopping the time loop (the output cadence of
+ * dns-const-q-xycut.c:489-516).  dnslbm_output_begin queues, on the
+ * context's stream ahead of any later step, the kernels that compute the
+ * requested outputs of the current state into device buffers -- the state
+ * as dnslbm_store_state writes it, vel/den as dnslbm_moments, the turb-fld
+ * rows as dnslbm_statistics -- and their copies into the caller's host
+ * buffers on a second stream, and returns at once: steps called after it
+ * run while the copies drain.  Any pointer may be NULL.  Host buffers should
+ * be page-locked (dnslbm_host_alloc) so that the copies overlap the steps;
+ * they must not be read or reused until dnslbm_output_wait returns.  Device
+ * buffers are allocated by the first call that needs them
+ * (DNSLBM_ERR_NOMEM if they do not fit) and kept; a new begin waits, on the
+ * device, for the previous copies. */
+int dnslbm_output_begin(dnslbm_ctx *ctx, double *state, double *vel, double *den, double *stats);
+/* Block until the copies of the last dnslbm_output_begin have landed. */
+int dnslbm_output_wait(dnslbm_ctx *ctx);
+
 /* Timing support for benchmarks: advance nsteps like dnslbm_step and return
  * CUDA-event times on the context's stream: total, and the summed device
  * time of the two step kernels (even / odd parity launches). */
