@@ -12,7 +12,7 @@
 
 #include "../../include/dnslbm.h"
 #include "step_common.cuh"
-#include "step_tma.cuh"
+#include "step_persist.cuh"
 
 namespace dnslbm {
 void launch_step_f64(const StepArgs &p, dim3 grid, dim3 block, bool odd, int tex, cudaStream_t s);
@@ -25,6 +25,26 @@ void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int row
 void launch_stats_sample(int nz, double np, const double *planes, double *mean, double *acc, bool accumulate,
                          cudaStream_t s);
 void launch_stats_rows(int nz, double np, const double *mean, const double *planes, double *out, cudaStream_t s);
+int persist_prepare_f64(size_t smem);
+int persist_occupancy_f64(int threads, size_t smem);
+cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s);
+int persist_prepare_lp(int precision, size_t smem);
+int persist_occupancy_lp(int precision, int threads, size_t smem);
+cudaError_t launch_persist_lp(int precision, const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s);
+static int persist_prepare(int precision, size_t smem)
+{
+    return precision == 64 ? persist_prepare_f64(smem) : persist_prepare_lp(precision, smem);
+}
+static int persist_occupancy_of(int precision, int threads, size_t smem)
+{
+    return precision == 64 ? persist_occupancy_f64(threads, smem) : persist_occupancy_lp(precision, threads, smem);
+}
+static cudaError_t launch_persist_batch(int precision, const PersistArgs &a, int grid, int threads, size_t smem,
+                                        cudaStream_t s)
+{
+    return precision == 64 ? launch_persist_f64(a, grid, threads, smem, s)
+                           : launch_persist_lp(precision, a, grid, threads, smem, s);
+}
 int tma_prepare_f64(size_t smem);
 int tma_occupancy_f64(int threads, size_t smem);
 void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
@@ -63,6 +83,7 @@ struct dnslbm_ctx {
     // planes of the row-pipelined kernel (nclean, ascending) followed by the
     // planes with link masks (ndirty), which a second launch steps per cell
     int *plane_list = nullptr;
+    std::vector<int> plane_host;  // host copy of plane_list
     int nclean = 0, ndirty = 0;
     LinksLaunch *d_llaunch = nullptr;  // the second launch's table (one entry)
     int tma_target = 0;                // resident blocks of the row-pipelined kernel
@@ -273,6 +294,7 @@ static cudaError_t upload_planes(dnslbm_ctx *c, const std::vector<int> *band = n
     for (int z = 0; z < c->nz; ++z)
         if (band && (*band)[z] >= 0) pl.push_back(z);
     c->ndirty = c->nz - c->nclean;
+    c->plane_host = pl;
     return cudaMemcpy(c->plane_list, pl.data(), pl.size() * sizeof(int), cudaMemcpyHostToDevice);
 }
 
@@ -1217,6 +1239,22 @@ struct dnslbm_batch {
     size_t smem = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // a chunk of steps starting on an even / odd parity
     int graph_steps = 32;
+    // the persistent kernel (default): one cooperative launch per chunk of
+    // steps, blocks taking items of work from a per-step counter
+    int persistent = 1;
+    int pgrid = 0;                      // its blocks (all resident)
+    size_t pstage = 0, psmem = 0;       // bytes of one stage, dynamic shared memory
+    std::vector<BatchItem> items;       // the items of one step, largest first
+    std::vector<BatchItem> items_uploaded;
+    BatchItem *d_items = nullptr;
+    size_t d_items_cap = 0;
+    unsigned *d_counters = nullptr;     // [graph_steps] items taken per step
+    unsigned *d_arrivals = nullptr;     // grid-barrier arrivals
+    int *d_abort = nullptr;             // a bounded wait of the launch gave up
+    int graph_ok = 1;                   // 0: stream capture of the cooperative launch was refused
+    int withhold = 0;                   // test hook: the next run withholds a load
+    unsigned long long withhold_wait_ns = 0;
+    char graph_note[160] = {0};
     size_t budget = 0;  // shared-memory budget per block the stages were sized for
     int stages = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -1262,6 +1300,10 @@ extern "C" void dnslbm_batch_destroy(dnslbm_batch *b)
         if (e) cudaEventDestroy(e);
     if (b->d_launch) cudaFree(b->d_launch);
     if (b->d_links) cudaFree(b->d_links);
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_counters) cudaFree(b->d_counters);
+    if (b->d_arrivals) cudaFree(b->d_arrivals);
+    if (b->d_abort) cudaFree(b->d_abort);
     for (auto &e : b->fj)
         if (e) cudaEventDestroy(e);
     if (b->side) cudaStreamDestroy(b->side);
@@ -1280,6 +1322,8 @@ constexpr size_t kBatchBudget1 = 220 * 1024, kBatchBudget2 = 108 * 1024, kBatchB
 // about the same number of cells, and the block count of the per-cell pass
 // over the planes with link masks.  A change of
 // either grid invalidates the captured graphs.
+static void persist_items(dnslbm_batch *b);
+
 static void batch_layout(dnslbm_batch *b)
 {
     // a common amount of work per block (cells of whole row groups), the
@@ -1319,6 +1363,86 @@ static void batch_layout(dnslbm_batch *b)
     b->grid = grid;
     b->links_blocks = lblocks;
     b->nlinks = nl;
+    if (b->persistent) persist_items(b);
+}
+
+// The items of one step of the persistent kernel: each plane of each
+// channel cut into runs of whole row groups (planes without link masks) or
+// of rows (planes with them) of about W cells, W chosen so that every
+// resident block takes about four items per step; largest first, so the
+// last items taken are the small ones.  An item's slot is its index within
+// its plane, so the plane sums do not depend on which block takes it.
+static void persist_items(dnslbm_batch *b)
+{
+    double total = 0;
+    for (auto *c : b->ch) total += (double)c->nx * c->ny * c->nz;
+    const double W = std::max(1.0, total / (4.0 * std::max(1, b->pgrid)));
+    std::vector<BatchItem> it;
+    std::vector<double> cells;
+    for (int ci = 0; ci < (int)b->ch.size(); ++ci) {
+        dnslbm_ctx *c = b->ch[ci];
+        const TmaArgs &t = c->tma;
+        for (int pi = 0; pi < c->nclean; ++pi) {
+            const double gcells = (double)t.k * c->nx;
+            const int per = std::max(1, (int)(W / gcells));
+            const int n = (t.gpp + per - 1) / per;
+            for (int j = 0; j < n; ++j) {
+                const int g0 = (int)((long long)t.gpp * j / n), g1 = (int)((long long)t.gpp * (j + 1) / n);
+                BatchItem x{};
+                x.chan = ci;
+                x.kind = 0;
+                x.first = pi * t.gpp + g0;
+                x.count = g1 - g0;
+                x.plane = c->plane_host[pi];
+                x.slot = j;
+                x.ncontrib = n;
+                it.push_back(x);
+                cells.push_back(std::min((double)(g1 - g0) * t.k, (double)c->ny) * c->nx);
+            }
+        }
+        for (int pi = c->nclean; pi < c->nz; ++pi) {
+            const int per = std::max(1, (int)(W / c->nx));
+            const int n = (c->ny + per - 1) / per;
+            for (int j = 0; j < n; ++j) {
+                BatchItem x{};
+                x.chan = ci;
+                x.kind = 1;
+                x.plane = c->plane_host[pi];
+                x.y0 = (int)((long long)c->ny * j / n);
+                x.y1 = (int)((long long)c->ny * (j + 1) / n);
+                x.slot = j;
+                x.ncontrib = n;
+                it.push_back(x);
+                cells.push_back((double)(x.y1 - x.y0) * c->nx);
+            }
+        }
+    }
+    std::vector<int> order(it.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cells[a] > cells[c]; });
+    b->items.resize(it.size());
+    for (size_t i = 0; i < order.size(); ++i) b->items[i] = it[order[i]];
+}
+
+// Shape of the persistent kernel for the current stages and consumers:
+// stage bytes of the largest channel, dynamic shared memory, resident grid.
+static int persist_configure(dnslbm_batch *b)
+{
+    size_t stage = 0;
+    for (auto *c : b->ch) stage = std::max(stage, (size_t)Q * c->tma.row_bytes * c->tma.k);
+    const size_t smem = persist_smem(b->stages, stage);
+    int maxsmem = 0, nsm = 0;
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+    const size_t cap = (size_t)maxsmem - kStaticSmemReserve;
+    if (smem > cap || nsm < 1) return -1;
+    const int occ = persist_prepare(b->precision, cap) ? 0 : persist_occupancy_of(b->precision, b->threads, smem);
+    cudaGetLastError();
+    if (occ < 1) return -1;
+    b->pstage = stage;
+    b->psmem = smem;
+    b->pgrid = occ * nsm;
+    return 0;
 }
 
 // One launch shape for all channels: per channel the most rows per stage
@@ -1366,6 +1490,7 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
     b->smem = smem;
     b->budget = budget;
     b->stages = stages;
+    if (b->persistent && persist_configure(b)) return -1;
     destroy_graphs(b);
     batch_layout(b);
     return 0;
@@ -1382,6 +1507,9 @@ extern "C" int dnslbm_batch_create(const dnslbm_deck *decks, int n, dnslbm_batch
     b = new dnslbm_batch();
     b->precision = decks[0].precision;
     b->device = decks[0].device;
+    // DNSLBM_BATCH=launch: one launch of the per-step batch kernel per step
+    // (the layout before the persistent kernel, kept for comparison)
+    if (const char *e = getenv("DNSLBM_BATCH")) b->persistent = strcmp(e, "launch") != 0;
     for (int i = 0; i < n; ++i) {
         dnslbm_ctx *c = nullptr;
         int rc = dnslbm_create(&decks[i], &c);
@@ -1418,7 +1546,10 @@ extern "C" int dnslbm_batch_create(const dnslbm_deck *decks, int n, dnslbm_batch
         cudaMalloc(&b->d_links, sizeof(LinksLaunch) * n) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->fj[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->fj[1], cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&b->fj[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&b->d_counters, sizeof(unsigned) * b->graph_steps) != cudaSuccess ||
+        cudaMalloc(&b->d_arrivals, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&b->d_abort, sizeof(int)) != cudaSuccess || cudaMemset(b->d_abort, 0, sizeof(int)) != cudaSuccess)
         return bail(bfail(b, DNSLBM_ERR_CUDA, "batch set-up failed: %s", cudaGetErrorString(cudaGetLastError())));
     *out = b;
     return DNSLBM_OK;
@@ -1455,6 +1586,69 @@ static int batch_launch(dnslbm_batch *b, bool odd)
         BCK(cudaStreamWaitEvent(b->stream, b->fj[1], 0));
     }
     BCK(cudaGetLastError());
+    return DNSLBM_OK;
+}
+
+// The persistent kernel's chunk of n steps from parity `odd`: counters and
+// barrier arrivals cleared, then one cooperative launch.
+static int persist_launch(dnslbm_batch *b, int n, int odd)
+{
+    PersistArgs a;
+    a.chans = b->d_launch;
+    a.items = b->d_items;
+    a.nitems = (int)b->items.size();
+    a.nsteps = n;
+    a.first_odd = odd;
+    a.stages = b->stages;
+    a.stage_bytes = (unsigned)b->pstage;
+    a.counters = b->d_counters;
+    a.arrivals = b->d_arrivals;
+    a.abort = b->d_abort;
+    a.wait_ns = b->withhold ? b->withhold_wait_ns : b->ch[0]->wait_ns;
+    a.withhold = b->withhold;
+    BCK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * n, b->stream));
+    BCK(cudaMemsetAsync(b->d_arrivals, 0, sizeof(unsigned), b->stream));
+    BCK(launch_persist_batch(b->precision, a, b->pgrid, b->threads, b->psmem, b->stream));
+    return DNSLBM_OK;
+}
+
+static int persist_run(dnslbm_batch *b, long nsteps)
+{
+    int odd = b->ch[0]->odd;
+    long left = nsteps;
+    BCK(cudaMemsetAsync(b->d_abort, 0, sizeof(int), b->stream));
+    while (left > 0) {
+        const int n = (int)std::min<long>(left, b->graph_steps);
+        if (n == b->graph_steps && b->graph_ok && !b->withhold) {
+            cudaGraphExec_t &g = b->graph[odd];
+            if (!g) {
+                // the time loop's chunk captured as a graph; a driver that
+                // refuses to capture the cooperative launch leaves plain
+                // launches (noted in the kernel description)
+                cudaGraph_t graph = nullptr;
+                BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+                const int rc = persist_launch(b, n, odd);
+                cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
+                if (rc == DNSLBM_OK && ee == cudaSuccess) ee = cudaGraphInstantiate(&g, graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                if (rc != DNSLBM_OK || ee != cudaSuccess) {
+                    cudaGetLastError();
+                    g = nullptr;
+                    b->graph_ok = 0;
+                    snprintf(b->graph_note, sizeof b->graph_note, " (graph capture refused: %s)",
+                             ee != cudaSuccess ? cudaGetErrorString(ee) : b->err);
+                    continue;
+                }
+            }
+            BCK(cudaGraphLaunch(g, b->stream));
+        } else {
+            const int rc = persist_launch(b, n, odd);
+            b->withhold = 0;
+            if (rc) return rc;
+        }
+        left -= n;
+        odd = (odd + n) & 1;
+    }
     return DNSLBM_OK;
 }
 
@@ -1499,9 +1693,33 @@ static int batch_run(dnslbm_batch *b, long nsteps, double *ms)
     if (!hl.empty())
         BCK(cudaMemcpyAsync(b->d_links, hl.data(), sizeof(LinksLaunch) * hl.size(), cudaMemcpyHostToDevice,
                             b->stream));
+    if (b->persistent) {
+        // the item table (a new one invalidates the captured graphs, which
+        // hold its address and length)
+        if (b->items.size() > b->d_items_cap) {
+            if (b->d_items) cudaFree(b->d_items);
+            b->d_items = nullptr;
+            b->d_items_cap = 0;
+            BCK(cudaMalloc(&b->d_items, sizeof(BatchItem) * b->items.size()));
+            b->d_items_cap = b->items.size();
+            destroy_graphs(b);
+        }
+        if (b->items.size() != b->items_uploaded.size() ||
+            memcmp(b->items.data(), b->items_uploaded.data(), sizeof(BatchItem) * b->items.size())) {
+            destroy_graphs(b);
+            b->items_uploaded = b->items;
+        }
+        BCK(cudaMemcpyAsync(b->d_items, b->items.data(), sizeof(BatchItem) * b->items.size(),
+                            cudaMemcpyHostToDevice, b->stream));
+    }
     int odd = b->ch[0]->odd;
     long left = nsteps;
     if (ms) BCK(cudaEventRecord(b->ev[0], b->stream));
+    if (b->persistent) {
+        const int rc = persist_run(b, nsteps);
+        if (rc) return rc;
+        left = 0;
+    }
     // the time loop: chunks of graph_steps launches replayed from a CUDA graph
     while (left >= b->graph_steps) {
         cudaGraphExec_t &g = b->graph[odd];
@@ -1538,6 +1756,15 @@ static int batch_run(dnslbm_batch *b, long nsteps, double *ms)
         c->done += nsteps;
         c->odd = (c->odd + (int)(nsteps & 1)) & 1;
     }
+    if (b->persistent) {
+        int ab = 0;
+        BCK(cudaMemcpy(&ab, b->d_abort, sizeof ab, cudaMemcpyDeviceToHost));
+        if (ab) {
+            for (auto *c : b->ch) c->have_state = 0;
+            return bfail(b, DNSLBM_ERR_TIMEOUT, "a bounded wait of the persistent batch kernel ran out; states "
+                                                "invalid, reload them");
+        }
+    }
     for (int i = 0; i < n; ++i) {
         int rc = check_status(b->ch[i]);
         if (rc) return bfail(b, rc, "channel %d: %s", i, b->ch[i]->err);
@@ -1557,10 +1784,28 @@ extern "C" int dnslbm_batch_step_timed(dnslbm_batch *b, long nsteps, double *ms)
     return batch_run(b, nsteps, ms);
 }
 
+extern "C" int dnslbm_batch_test_withhold_load(dnslbm_batch *b, double wait_ms)
+{
+    if (!b) return bfail(b, DNSLBM_ERR_ARG, "null batch");
+    if (!b->persistent) return bfail(b, DNSLBM_ERR_STATE, "the batch steps with one launch per step");
+    if (!(wait_ms > 0.0 && wait_ms <= 600000.0)) return bfail(b, DNSLBM_ERR_ARG, "wait limit %g ms out of range", wait_ms);
+    b->withhold = 1;
+    b->withhold_wait_ns = (unsigned long long)(wait_ms * 1e6);
+    return DNSLBM_OK;
+}
+
 extern "C" const char *dnslbm_batch_kernel(const dnslbm_batch *b)
 {
-    static thread_local char buf[256];
+    static thread_local char buf[384];
     if (!b) return "";
+    if (b->persistent) {
+        snprintf(buf, sizeof buf,
+                 "persist_batch_kernel<fp%d>: %zu channels, %zu items per step, %d blocks x %d threads, %d stages, "
+                 "%zu B smem; one cooperative launch per %d steps, CUDA graph%s",
+                 b->precision, b->ch.size(), b->items.size(), b->pgrid, b->threads, b->stages, b->psmem,
+                 b->graph_steps, b->graph_note);
+        return buf;
+    }
     snprintf(buf, sizeof buf, "step_tma_batch_kernel<fp%d>: %zu channels, %d blocks x %d threads, %d stages, %zu B smem"
              "%s%s; CUDA graph of %d steps", b->precision, b->ch.size(), b->grid, b->threads, b->stages, b->smem,
              b->links_blocks ? " + links_pass_kernel: " : "",

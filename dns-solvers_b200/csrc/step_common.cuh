@@ -222,7 +222,8 @@ static __device__ __forceinline__ void step_tail(const StepArgs &a, long long st
 #pragma unroll
         for (int i = 0; i < NP; ++i) s[i] = __ldcg(ps + i);
         const double um = s[2] / np, vm = s[3] / np, wm = s[4] / np;
-        const double du = um - cshift[z * 3 + 0], dv = vm - cshift[z * 3 + 1], dw = wm - cshift[z * 3 + 2];
+        const double du = um - __ldcg(cshift + z * 3 + 0), dv = vm - __ldcg(cshift + z * 3 + 1),
+                     dw = wm - __ldcg(cshift + z * 3 + 2);
         t[0] += s[0];
         t[1] += s[1];
         t[2] += um;
@@ -261,7 +262,7 @@ static __device__ __forceinline__ void step_tail(const StepArgs &a, long long st
     rec[6] = stdown;
     rec[7] = stress;
     rec[8] = force_used * nz / 2.;
-    if (stress != stress && a.status[0] == 0) a.status[0] = step + 1;
+    if (stress != stress && __ldcg(a.status) == 0) a.status[0] = step + 1;
     // constant-Q: next force from the totals of the state this step wrote
     // (encalc.c:121 evaluated one step ahead); sum of populations = t[4]
     a.force[(step + 1) & 1] = a.const_q ? (t[4] / N) * a.ubulk - t[5] / N : a.gx;

@@ -1,0 +1,366 @@
+// Batched channels in one persistent launch.
+//
+// One cooperative launch (every block resident at once) advances all
+// channels of a batch through nsteps time steps.  Within a step the work is
+// a table of items, largest first:
+//   kind 0  a run of row groups of one plane of one channel, moved through
+//           the block's shared-memory stages by the bulk-copy engine and
+//           collided by the consumer warps (the row-pipelined step of
+//           step_tma.cuh);
+//   kind 1  the cells of some rows of a plane with per-cell link masks
+//           (solids inside the flow), collided by the consumer warps from
+//           global memory (links_cell).
+// A block's producer warp takes the next item from the step's counter
+// (atomicAdd), so blocks that drew small items take more: no block waits
+// for a channel it owns.  Each item sums its cells into its own partial-sum
+// slot of its plane (the item's index within the plane), so the plane sums,
+// the logs and the next force do not depend on which block took which item.
+// The last item of a channel's step runs that channel's step tail.  Steps
+// are separated by a grid-wide barrier.
+//
+// Every wait is bounded by the GPU's global timer: the stage waits (as in
+// step_tma.cuh) and the grid barrier.  A wait that runs out raises the
+// launch's abort flag: the block's consumers leave the step together (one
+// barrier-reduction per stage makes that decision uniform), its producer
+// waits for the copies it has issued, every block still arrives at the
+// grid barrier, and no block starts another step.
+//
+// Memory written by other SMs earlier in the launch is read through L2:
+// bulk copies always are; the per-thread loads use ld.global.cg, and the
+// per-channel force, plane means and step counter are read with __ldcg.
+#pragma once
+
+#include "step_tma.cuh"
+
+namespace dnslbm {
+
+struct BatchItem {
+    int chan;            // index into the channel table
+    int kind;            // 0: row groups through the stages, 1: cells of a plane with link masks
+    int first, count;    // kind 0: row groups first .. first+count-1 (channel's group numbering)
+    int plane;           // kind 1: the plane z
+    int y0, y1;          // kind 1: rows y0 .. y1-1
+    int slot, ncontrib;  // partial-sum slot of the item in its plane, items of that plane
+};
+
+struct PersistArgs {
+    const ChannelLaunch *chans;
+    const BatchItem *items;
+    int nitems, nsteps, first_odd, stages;
+    unsigned stage_bytes;          // bytes of one stage (the largest channel's)
+    unsigned *counters;            // [nsteps] items taken in each step (zero at launch)
+    unsigned *arrivals;            // grid-barrier arrivals (zero at launch)
+    int *abort;                    // a bounded wait gave up: the launch stops
+    unsigned long long wait_ns;    // limit of every bounded wait
+    int withhold;                  // test switch (0 otherwise): block 0 withholds its first load
+};
+
+// Shared memory after the stages: full[S], empty[S] (8 bytes each) and the
+// stage headers hdr[S][2] (item, row group within the item; item -1 ends
+// the step, row group -1 marks a kind-1 item).
+__host__ __device__ constexpr size_t persist_smem(int stages, size_t stage_bytes)
+{
+    return (size_t)stages * stage_bytes + 16 * (size_t)stages + 8 * (size_t)stages;
+}
+
+// OR of v over the first nthreads threads (named barrier 2): every one of
+// them gets the same answer at the same point.
+__device__ __forceinline__ bool consumers_any(int v, int nthreads)
+{
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.s32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 2, %2, q;\n\t"
+        "selp.s32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"(v), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+__device__ __forceinline__ void persist_raise(const PersistArgs &a, volatile int *s_abort)
+{
+    *s_abort = 1;
+    atomicExch(a.abort, 1);
+}
+
+template <typename T, bool ODD>
+__device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, int lane, unsigned char *smem,
+                                                 uint64_t *full, uint64_t *empty, int *hdr, volatile int *s_abort)
+{
+    const int S = a.stages;
+    int i = 0;            // stage sequence number within the step
+    // test switch: block 0 neither arms nor loads its first row group of the
+    // first step, so its consumers' wait runs out with no copy in flight
+    bool withhold = a.withhold != 0 && blockIdx.x == 0 && s == 0;
+    unsigned loaded = 0;  // bit st: a load into stage st was issued (its phase is the last one armed)
+    unsigned phase = 0;   // bit st: parity of that phase
+    // once the consumers have released sequence seq, store the row group it held
+    auto store_seq = [&](int seq) {
+        const int st = seq % S;
+        if (!*s_abort && !mbar_wait_bounded(empty + st, (uint32_t)((seq / S) & 1), a.wait_ns, s_abort))
+            persist_raise(a, s_abort);
+        const int h = hdr[2 * st], g = hdr[2 * st + 1];
+        if (*s_abort || h < 0 || g < 0 || lane >= Q) return;
+        const BatchItem it = a.items[h];
+        const ChannelLaunch &L = a.chans[it.chan];
+        int z, y0;
+        group_origin(L.t, it.first + g, z, y0);
+        const int k = min(L.t.k, L.p.ny - y0);
+        const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
+        const GroupRows gr = L.textured ? group_rows<ODD, 1>(L.p, lane, y0, z, wall)
+                                        : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
+        const size_t dir_bytes = (size_t)L.t.k * L.t.row_bytes;
+        if (gr.bulk) copy_group<T>(L.p, L.t, gr, k, smem + (size_t)st * a.stage_bytes + lane * dir_bytes, false, nullptr);
+        bulk_commit();
+    };
+    // the stage of sequence i, free for new contents
+    auto next_stage = [&]() {
+        if (i >= S) store_seq(i - S);
+        if (lane < Q) bulk_wait_read_all();  // this lane's store of the stage has read it
+        __syncwarp();
+        return i % S;
+    };
+    for (;;) {
+        int h = 0;
+        if (lane == 0) h = *s_abort ? a.nitems : (int)atomicAdd(a.counters + s, 1u);
+        h = __shfl_sync(0xffffffffu, h, 0);
+        if (h >= a.nitems) break;
+        const BatchItem it = a.items[h];
+        if (it.kind == 1) {  // no copies: the consumers work from global memory
+            const int st = next_stage();
+            if (lane == 0) {
+                hdr[2 * st] = h;
+                hdr[2 * st + 1] = -1;
+                mbar_arrive(full + st);
+            }
+            __syncwarp();
+            ++i;
+            continue;
+        }
+        const ChannelLaunch &L = a.chans[it.chan];
+        const size_t dir_bytes = (size_t)L.t.k * L.t.row_bytes;
+        for (int g = 0; g < it.count; ++g) {
+            const int st = next_stage();
+            int z, y0;
+            group_origin(L.t, it.first + g, z, y0);
+            const int k = min(L.t.k, L.p.ny - y0);
+            const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
+            GroupRows gr{};
+            if (lane < Q)
+                gr = L.textured ? group_rows<ODD, 1>(L.p, lane, y0, z, wall) : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
+            const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && gr.bulk);
+            const bool issue = __shfl_sync(0xffffffffu, *s_abort, 0) == 0 && !withhold;
+            withhold = false;
+            if (issue) {
+                if (lane == 0) {
+                    hdr[2 * st] = h;
+                    hdr[2 * st + 1] = g;
+                    mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * L.t.row_bytes));
+                }
+                __syncwarp();
+                if (lane < Q && gr.bulk)
+                    copy_group<T>(L.p, L.t, gr, k, smem + (size_t)st * a.stage_bytes + lane * dir_bytes, true, full + st);
+                loaded |= 1u << st;
+                phase = (phase & ~(1u << st)) | ((unsigned)((i / S) & 1) << st);
+            }
+            ++i;
+        }
+    }
+    {  // end of the step
+        const int st = next_stage();
+        if (lane == 0) {
+            hdr[2 * st] = -1;
+            mbar_arrive(full + st);
+        }
+        __syncwarp();
+        ++i;
+    }
+    for (int seq = max(0, i - S); seq < i - 1; ++seq) store_seq(seq);
+    if (lane < Q) bulk_wait_all();
+    if (*s_abort)  // loads still landing in shared memory (bounded; an issued load completes)
+        for (int st = 0; st < S; ++st)
+            if ((loaded >> st) & 1u) mbar_wait_bounded(full + st, (phase >> st) & 1u, a.wait_ns, nullptr);
+}
+
+// Kind-1 item: the cells of rows y0..y1-1 of a plane with link masks, one
+// thread per cell.
+template <typename T, bool ODD, bool CONSTQ>
+__device__ __forceinline__ void persist_links(const StepArgs &p, const BatchItem &it, double G, const double (&sh)[3],
+                                              double (&acc)[NP], int nc)
+{
+    const int z = it.plane, nx = p.nx;
+    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const int ncell = (it.y1 - it.y0) * nx;
+    for (int c = threadIdx.x; c < ncell; c += nc) {
+        const int dy = c / nx, x = c - dy * nx, y = it.y0 + dy;
+        float racc[NP];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) racc[q] = 0.f;
+        const Nbr n = make_nbr(x, y, z, nx, p.ny, p.pitch);
+        links_cell<T, ODD, CONSTQ>(p, n, wall, cell_links(p.band_of, p.links, nx, p.ny, x, y, z), nullptr, 0, G,
+                                   sh[0], sh[1], sh[2], acc, racc);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) acc[q] += (double)racc[q];
+    }
+}
+
+template <typename T, bool ODD>
+__device__ __forceinline__ void persist_consumers(const PersistArgs &a, unsigned char *smem, uint64_t *full,
+                                                  uint64_t *empty, const int *hdr, int nc, volatile int *s_abort)
+{
+    using LpT = typename std::conditional<std::is_same<T, double>::value, float, T>::type;
+    const int S = a.stages;
+    double acc[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) acc[q] = 0.0;
+    for (int i = 0;; ++i) {
+        const int st = i % S;
+        int bad = 0;
+        if (!*s_abort && !mbar_wait_bounded(full + st, (uint32_t)((i / S) & 1), a.wait_ns, s_abort)) bad = 1;
+        if (consumers_any(bad | *s_abort, nc)) {  // every consumer leaves the step here together
+            if (threadIdx.x == 0) persist_raise(a, s_abort);
+            return;
+        }
+        const int h = hdr[2 * st], g = hdr[2 * st + 1];
+        if (h < 0) return;  // end of the step (the same header for every consumer)
+        const BatchItem it = a.items[h];
+        const ChannelLaunch &L = a.chans[it.chan];
+        const StepArgs &p = L.p;
+        const bool q = p.const_q != 0;
+        const long long step = __ldcg(p.step_ctr);
+        const double G = q ? __ldcg(p.force + (step & 1)) : p.gx;
+        int z, y0 = 0;
+        if (it.kind == 1) z = it.plane;
+        else group_origin(L.t, it.first + g, z, y0);
+        const double *shp = p.shift + (size_t)(step & 1) * p.nz * 3 + z * 3;
+        const double sh[3] = {__ldcg(shp), __ldcg(shp + 1), __ldcg(shp + 2)};
+        if (it.kind == 1) {
+            if (q) persist_links<T, ODD, true>(p, it, G, sh, acc, nc);
+            else persist_links<T, ODD, false>(p, it, G, sh, acc, nc);
+        } else {
+            const int k = min(L.t.k, p.ny - y0);
+            const int dstride = L.t.k * p.pitch;
+            T *sb = reinterpret_cast<T *>(smem + (size_t)st * a.stage_bytes);
+            [[maybe_unused]] const LpParams lk = lp_params<LpT>((float)p.omega, (float)G);
+            if (q) {
+                if (L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
+                else consume_group<T, ODD, true, false>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
+            } else {
+                if (L.textured) consume_group<T, ODD, false, true>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
+                else consume_group<T, ODD, false, false>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
+            }
+            fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
+        }
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);
+        if (it.kind == 1 || g == it.count - 1) {  // the item is done: its plane contribution
+            plane_contribute(p, acc, z, it.slot, it.ncontrib, step, G, 0, nc);
+#pragma unroll
+            for (int r = 0; r < NP; ++r) acc[r] = 0.0;
+        }
+    }
+}
+
+template <typename T, bool ODD>
+__device__ __forceinline__ void persist_step(const PersistArgs &a, int s, unsigned char *smem, volatile int *s_abort)
+{
+    const int S = a.stages, nc = blockDim.x - 32;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * a.stage_bytes);
+    uint64_t *empty = full + S;
+    int *hdr = reinterpret_cast<int *>(empty + S);
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < S; ++st) {
+            mbar_init(full + st, 1);
+            mbar_init(empty + st, nc / 32);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x >= nc) persist_producer<T, ODD>(a, s, threadIdx.x - nc, smem, full, empty, hdr, s_abort);
+    else persist_consumers<T, ODD>(a, smem, full, empty, hdr, nc, s_abort);
+}
+
+// Grid-wide barrier between steps (all blocks are resident: cooperative
+// launch).  Bounded: gives up after wait_ns, raising the abort flag.
+// Returns false when the launch is to stop.
+__device__ __forceinline__ bool persist_grid_barrier(const PersistArgs &a, unsigned target)
+{
+    __shared__ int s_go;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fence_async_global();  // this block's bulk stores before its arrival
+        __threadfence();
+        atomicAdd(a.arrivals, 1u);
+        int go = !*(volatile int *)a.abort;
+        const unsigned long long t0 = globaltimer_ns();
+        while (go && *(volatile unsigned *)a.arrivals < target) {
+            if (*(volatile int *)a.abort) go = 0;
+            else if (globaltimer_ns() - t0 > a.wait_ns) {
+                atomicExch(a.abort, 1);
+                go = 0;
+            } else {
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        fence_async_global();  // the other blocks' stores before this block's next loads
+        s_go = go && !*(volatile int *)a.abort;
+    }
+    __syncthreads();
+    return s_go != 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTmaMaxThreads, 1) persist_batch_kernel(const PersistArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_abort;
+    for (int s = 0; s < a.nsteps; ++s) {
+        if (threadIdx.x == 0) s_abort = 0;
+        if ((a.first_odd + s) & 1) persist_step<T, true>(a, s, smem, &s_abort);
+        else persist_step<T, false>(a, s, smem, &s_abort);
+        if (!persist_grid_barrier(a, (unsigned)(s + 1) * gridDim.x)) break;
+    }
+}
+
+template <typename T>
+int persist_set_smem_attr(size_t bytes)
+{
+    return cudaFuncSetAttribute(persist_batch_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
+                   cudaSuccess
+               ? 0
+               : -1;
+}
+
+template <typename T>
+int persist_occupancy(int threads, size_t smem)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persist_batch_kernel<T>, threads, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+// Cooperative launch: fails (instead of deadlocking) when the grid cannot
+// be resident at once.
+template <typename T>
+cudaError_t launch_persist(const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, persist_batch_kernel<T>, a);
+}
+
+}  // namespace dnslbm

@@ -568,6 +568,30 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
 
 constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer warp
 
+// The consumers' work on one row group in a stage: FP64 one cell per thread
+// and iteration in the reference's operand order; FP32/FP16 cell pairs on
+// the packed FP32 pipe, except the planes next to a textured wall.
+template <typename T, bool ODD, bool CONSTQ, bool TXT>
+__device__ __forceinline__ void consume_group(const StepArgs &p, const LpParams &lk, T *sb, int dstride, int y0, int k,
+                                              int z, double G, const double *sh, double (&acc)[NP], int nc)
+{
+    if constexpr (std::is_same<T, double>::value) {
+        if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        else if (z == p.nz - 1) tma_group<T, ODD, CONSTQ, TXT, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        else tma_group<T, ODD, CONSTQ, TXT, 0>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+    } else {
+        if (z == 0) {
+            if (TXT) tma_group<T, ODD, CONSTQ, true, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+            else tma_group2<T, ODD, CONSTQ, -1>(p, lk, sb, dstride, k, sh, acc, nc);
+        } else if (z == p.nz - 1) {
+            if (TXT) tma_group<T, ODD, CONSTQ, true, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+            else tma_group2<T, ODD, CONSTQ, 1>(p, lk, sb, dstride, k, sh, acc, nc);
+        } else {
+            tma_group2<T, ODD, CONSTQ, 0>(p, lk, sb, dstride, k, sh, acc, nc);
+        }
+    }
+}
+
 // The step of one channel by one block: `blk` numbers the block among the
 // channel's blocks, `tma_smem` is the block's dynamic shared memory.
 template <typename T, bool ODD, bool CONSTQ, int TEX>
@@ -616,23 +640,7 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
             atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
         }
         T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
-        const double *sh = shift_now + z * 3;
-        constexpr bool TXT = TEX != 0;
-        if constexpr (std::is_same<T, double>::value) {
-            if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-            else if (z == p.nz - 1) tma_group<T, ODD, CONSTQ, TXT, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-            else tma_group<T, ODD, CONSTQ, TXT, 0>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-        } else {
-            if (z == 0) {
-                if (TXT) tma_group<T, ODD, CONSTQ, true, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-                else tma_group2<T, ODD, CONSTQ, -1>(p, lk, sb, dstride, k, sh, acc, nc);
-            } else if (z == p.nz - 1) {
-                if (TXT) tma_group<T, ODD, CONSTQ, true, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-                else tma_group2<T, ODD, CONSTQ, 1>(p, lk, sb, dstride, k, sh, acc, nc);
-            } else {
-                tma_group2<T, ODD, CONSTQ, 0>(p, lk, sb, dstride, k, sh, acc, nc);
-            }
-        }
+        consume_group<T, ODD, CONSTQ, TEX != 0>(p, lk, sb, dstride, y0, k, z, G, shift_now + z * 3, acc, nc);
         fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);

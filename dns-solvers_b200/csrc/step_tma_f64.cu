@@ -1,6 +1,7 @@
-// FP64 instantiation of the row-pipelined step (step_tma.cuh).  Compiled
-// with -fmad=false: the collision keeps the reference's rounding.
-#include "step_tma.cuh"
+// FP64 instantiation of the row-pipelined step (step_tma.cuh) and of the
+// persistent batch kernel (step_persist.cuh).  Compiled with -fmad=false: the
+// collision keeps the reference's rounding.
+#include "step_persist.cuh"
 
 namespace dnslbm {
 
@@ -24,6 +25,13 @@ void launch_tma_batch_f64(const ChannelLaunch *chans, int nchan, int grid, int t
 void launch_links_f64(const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s)
 {
     launch_links_pass<double>(tab, n, blocks, odd, s);
+}
+
+int persist_prepare_f64(size_t smem) { return persist_set_smem_attr<double>(smem); }
+int persist_occupancy_f64(int threads, size_t smem) { return persist_occupancy<double>(threads, smem); }
+cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s)
+{
+    return launch_persist<double>(a, grid, threads, smem, s);
 }
 
 }  // namespace dnslbm

@@ -1,5 +1,6 @@
-// FP32 / FP16 instantiations of the row-pipelined step (step_tma.cuh).
-#include "step_tma.cuh"
+// FP32 / FP16 instantiations of the row-pipelined step (step_tma.cuh) and of
+// the persistent batch kernel (step_persist.cuh).
+#include "step_persist.cuh"
 
 namespace dnslbm {
 
@@ -38,6 +39,20 @@ void launch_links_lp(int precision, const LinksLaunch *tab, int n, int blocks, b
 {
     if (precision == 32) launch_links_pass<float>(tab, n, blocks, odd, s);
     else launch_links_pass<__half>(tab, n, blocks, odd, s);
+}
+
+int persist_prepare_lp(int precision, size_t smem)
+{
+    return precision == 32 ? persist_set_smem_attr<float>(smem) : persist_set_smem_attr<__half>(smem);
+}
+int persist_occupancy_lp(int precision, int threads, size_t smem)
+{
+    return precision == 32 ? persist_occupancy<float>(threads, smem) : persist_occupancy<__half>(threads, smem);
+}
+cudaError_t launch_persist_lp(int precision, const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s)
+{
+    return precision == 32 ? launch_persist<float>(a, grid, threads, smem, s)
+                           : launch_persist<__half>(a, grid, threads, smem, s);
 }
 
 }  // namespace dnslbm

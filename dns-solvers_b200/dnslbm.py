@@ -100,6 +100,7 @@ def lib():
     L.dnslbm_batch_kernel.argtypes = [vp]
     L.dnslbm_batch_kernel.restype = ctypes.c_char_p
     L.dnslbm_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    L.dnslbm_batch_test_withhold_load.argtypes = [vp, ctypes.c_double]
     L.dnslbm_host_alloc.argtypes = [ctypes.c_size_t]
     L.dnslbm_host_alloc.restype = vp
     L.dnslbm_host_free.argtypes = [vp]
@@ -305,8 +306,8 @@ def deck(xdv, ydv, zdv, omega, ubulk=0.0, gx=0.0, force_mode=CONST_G, precision=
 
 
 class Batch:
-    """Many independent channels stepped by one launch per step, the time
-    loop replayed from a CUDA graph (dnslbm_batch_*)."""
+    """Many independent channels stepped together by the persistent batch
+    kernel, the time loop replayed from a CUDA graph (dnslbm_batch_*)."""
 
     def __init__(self, decks):
         self.L = lib()
@@ -334,6 +335,10 @@ class Batch:
     @property
     def kernel(self):
         return self.L.dnslbm_batch_kernel(self.h).decode()
+
+    def test_withhold_load(self, wait_ms=1.0):
+        """Test hook: the next step call withholds one load (ERR_TIMEOUT)."""
+        self._ck(self.L.dnslbm_batch_test_withhold_load(self.h, wait_ms))
 
     def autotune(self, steps=8):
         """Pick the fastest launch shape on rest states; before any load."""

@@ -226,11 +226,15 @@ void *dnslbm_host_alloc(size_t bytes);
 void dnslbm_host_free(void *ptr);
 
 /* Batched channels: many independent channels (own grid, walls, force,
- * state and logs) advanced together, one kernel launch per step for all of
- * them, the time loop replayed from a CUDA graph in chunks of 32 steps.  All
- * decks share one precision and device.  Use dnslbm_batch_channel(b, i) with
- * the single-channel calls (flags, load/store, logs, statistics) between
- * batch steps.  No counterpart in the reference (one channel per run). */
+ * state and logs) advanced together by one persistent kernel: one
+ * cooperative launch runs a chunk of 32 steps (the time loop, replayed from
+ * a CUDA graph), its blocks taking items of work -- runs of row groups, and
+ * the cells of planes next to solids -- from a per-step counter, largest
+ * first, with a bounded grid-wide barrier between steps.  All decks share
+ * one precision and device.  Use dnslbm_batch_channel(b, i) with the
+ * single-channel calls (flags, load/store, logs, statistics) between batch
+ * steps.  The environment variable DNSLBM_BATCH=launch selects one launch
+ * per step instead.  No counterpart in the reference (one channel per run). */
 typedef struct dnslbm_batch dnslbm_batch;
 int dnslbm_batch_create(const dnslbm_deck *decks, int n, dnslbm_batch **out);
 void dnslbm_batch_destroy(dnslbm_batch *b);
@@ -242,6 +246,12 @@ dnslbm_ctx *dnslbm_batch_channel(dnslbm_batch *b, int i);
 int dnslbm_batch_step(dnslbm_batch *b, long nsteps);
 /* The same, returning the device time of the whole batch in ms. */
 int dnslbm_batch_step_timed(dnslbm_batch *b, long nsteps, double *ms);
+/* Test hook for the persistent kernel's bounded waits (no counterpart in
+ * the reference): the next dnslbm_batch_step has its first block withhold
+ * its first load, with waits limited to wait_ms; the call returns
+ * DNSLBM_ERR_TIMEOUT and the channels need a new state.  DNSLBM_ERR_STATE
+ * when the batch steps with one launch per step. */
+int dnslbm_batch_test_withhold_load(dnslbm_batch *b, double wait_ms);
 /* Launch shape of the batched kernel. */
 const char *dnslbm_batch_kernel(const dnslbm_batch *b);
 /* Time the batched kernel's launch shapes (shared-memory budget for 1-3
