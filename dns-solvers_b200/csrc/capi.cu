@@ -26,31 +26,33 @@ void launch_stats_sample(int nz, double np, const double *planes, double *mean, 
                          cudaStream_t s);
 void launch_stats_rows(int nz, double np, const double *mean, const double *planes, double *out, cudaStream_t s);
 int persist_prepare_f64(size_t smem);
-int persist_occupancy_f64(int threads, size_t smem);
-cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s);
+int persist_occupancy_f64(int threads, size_t smem, bool any_q);
+cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, bool any_q, cudaStream_t s);
 int persist_prepare_lp(int precision, size_t smem);
-int persist_occupancy_lp(int precision, int threads, size_t smem);
-cudaError_t launch_persist_lp(int precision, const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s);
+int persist_occupancy_lp(int precision, int threads, size_t smem, bool any_q);
+cudaError_t launch_persist_lp(int precision, const PersistArgs &a, int grid, int threads, size_t smem, bool any_q,
+                              cudaStream_t s);
 static int persist_prepare(int precision, size_t smem)
 {
     return precision == 64 ? persist_prepare_f64(smem) : persist_prepare_lp(precision, smem);
 }
-static int persist_occupancy_of(int precision, int threads, size_t smem)
+static int persist_occupancy_of(int precision, int threads, size_t smem, bool any_q)
 {
-    return precision == 64 ? persist_occupancy_f64(threads, smem) : persist_occupancy_lp(precision, threads, smem);
+    return precision == 64 ? persist_occupancy_f64(threads, smem, any_q)
+                           : persist_occupancy_lp(precision, threads, smem, any_q);
 }
 static cudaError_t launch_persist_batch(int precision, const PersistArgs &a, int grid, int threads, size_t smem,
-                                        cudaStream_t s)
+                                        bool any_q, cudaStream_t s)
 {
-    return precision == 64 ? launch_persist_f64(a, grid, threads, smem, s)
-                           : launch_persist_lp(precision, a, grid, threads, smem, s);
+    return precision == 64 ? launch_persist_f64(a, grid, threads, smem, any_q, s)
+                           : launch_persist_lp(precision, a, grid, threads, smem, any_q, s);
 }
 int tma_prepare_f64(size_t smem);
-int tma_occupancy_f64(int threads, size_t smem);
+int tma_occupancy_f64(int threads, size_t smem, bool const_q);
 void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
                     cudaStream_t s);
 int tma_prepare_lp(int precision, size_t smem);
-int tma_occupancy_lp(int precision, int threads, size_t smem);
+int tma_occupancy_lp(int precision, int threads, size_t smem, bool const_q);
 void launch_tma_lp(int precision, const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd,
                    int tex, cudaStream_t s);
 int tma_batch_prepare_f64(size_t smem);
@@ -235,12 +237,18 @@ static void tma_layout(dnslbm_ctx *c)
     c->tma_grid = (ngroups + GB - 1) / GB;
 }
 
-static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bps)
+// seg > 0 (FP64 only): groups are x-segments of seg elements (even) of one
+// row, for rows too long for two whole-row stages.
+static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bps, int seg = 0)
 {
     const int row_bytes = c->pitch * (int)c->esize;
     k = std::max(1, std::min(k, c->ny));
     consumers = std::max(32, std::min(352, consumers / 32 * 32));
-    const size_t smem_stage = (size_t)Q * row_bytes * k;
+    if (seg > 0 && (c->deck.precision != 64 || seg % 2 || seg >= c->nx)) return -1;
+    if (seg > 0) k = 1;
+    const int nseg = seg > 0 ? (c->nx + seg - 1) / seg : 1;
+    const int dir_elems = seg > 0 ? seg + 4 : k * c->pitch;  // a segment keeps a halo of 2 elements a side
+    const size_t smem_stage = (size_t)Q * dir_elems * c->esize;
     int maxsmem = 0, nsm = 0;
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->deck.device);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->deck.device);
@@ -248,24 +256,28 @@ static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bp
     const size_t cap = (size_t)maxsmem - kStaticSmemReserve;  // room for the kernels' static shared memory
     if (stages < 2 || smem > cap || nsm <= 0) return -1;
     const int threads = consumers + 32;
+    const bool const_q = c->deck.force_mode == DNSLBM_FORCE_CONST_Q;
     // the kernels may use up to the device's opt-in shared memory (a batch can
     // give a channel a larger stage than its own shape)
     const int prep = c->deck.precision == 64 ? tma_prepare_f64(cap) : tma_prepare_lp(c->deck.precision, cap);
     int occ = prep ? 0
-                   : (c->deck.precision == 64 ? tma_occupancy_f64(threads, smem)
-                                              : tma_occupancy_lp(c->deck.precision, threads, smem));
+                   : (c->deck.precision == 64 ? tma_occupancy_f64(threads, smem, const_q)
+                                              : tma_occupancy_lp(c->deck.precision, threads, smem, const_q));
     cudaGetLastError();  // a failed query only rules the configuration out
     if (bps > 0) occ = std::min(occ, bps);
     if (occ < 1) return -1;
-    const int gpp = (c->ny + k - 1) / k;
+    const int gpp = (c->ny + k - 1) / k * nseg;
     c->use_tma = 1;
     c->tma_threads = threads;
     c->tma_smem = smem;
     c->tma_target = occ * nsm;
-    c->tma = TmaArgs{0, 1, stages, row_bytes, k, gpp, nullptr};
+    c->tma = TmaArgs{0, 1, stages, row_bytes, k, gpp, nullptr, nseg, seg > 0 ? seg : c->nx, dir_elems};
     tma_layout(c);
     return 0;
 }
+
+// x-segment length (even) that splits rows of nx into nseg near-equal parts.
+static int segment_for(int nx, int nseg) { return ((nx + nseg - 1) / nseg + 1) & ~1; }
 
 static void describe_kernel(dnslbm_ctx *c)
 {
@@ -275,6 +287,9 @@ static void describe_kernel(dnslbm_ctx *c)
                          "rows/block, %d stages, %zu B smem",
                          c->deck.precision, c->tma_grid, c->tma_threads, c->tma.groups_per_block, c->tma.k,
                          c->tma.stages, c->tma_smem);
+        if (c->tma.nseg > 1 && m > 0 && m < (int)sizeof c->kernel_desc)
+            m += snprintf(c->kernel_desc + m, sizeof c->kernel_desc - m, ", rows in %d x-segments of %d", c->tma.nseg,
+                          c->tma.seg);
         if (c->ndirty > 0 && m > 0 && m < (int)sizeof c->kernel_desc)
             snprintf(c->kernel_desc + m, sizeof c->kernel_desc - m, " + links_pass_kernel over %d planes", c->ndirty);
     } else {
@@ -376,7 +391,16 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         if (const char *e = getenv("DNSLBM_THREADS")) consumers = atoi(e) / 32 * 32;
         int bps = 0;
         if (const char *e = getenv("DNSLBM_BLOCKS_PER_SM")) bps = atoi(e);
-        if (!(path && !strcmp(path, "scalar"))) tma_configure(c, k, stages, consumers, bps);
+        if (!(path && !strcmp(path, "scalar"))) {
+            int seg = 0;
+            if (const char *e = getenv("DNSLBM_SEGMENT")) seg = atoi(e) & ~1;
+            if (seg > 0 || tma_configure(c, k, stages, consumers, bps)) {
+                // FP64 rows too long for two whole-row stages: x-segments
+                for (int nseg = 2; seg == 0 && c->deck.precision == 64 && nseg <= 8; ++nseg)
+                    if (!tma_configure(c, 1, stages, consumers, bps, segment_for(c->nx, nseg))) break;
+                if (seg > 0) tma_configure(c, 1, stages, consumers, bps, seg);
+            }
+        }
         describe_kernel(c);
     }
     // partial-sum slots: enough for the per-thread kernels and for any row
@@ -1197,18 +1221,30 @@ extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t re
     // the consumer count for the best pair
     const int cap = c->deck.precision == 64 ? 320 : (c->deck.precision == 32 ? 192 : 128);
     const int cons0 = std::min(cap, (c->nx + 31) / 32 * 32);
-    int bk = -1, bs = -1;
+    int bk = -1, bs = -1, bseg = 0;
     for (int k : {1, 2, 4, 8})
         for (int st : {2, 3, 4}) {
             if (k > c->ny || tma_configure(c, k, st, cons0, 0)) continue;
             double ms;
             if ((rc = time_choice(c, steps, &ms))) return rc;
             ++ncand;
-            if (ms < best_ms) best_ms = ms, best = save_choice(c), bk = k, bs = st;
+            if (ms < best_ms) best_ms = ms, best = save_choice(c), bk = k, bs = st, bseg = 0;
         }
+    // FP64 rows as x-segments (the only bulk-copy form for rows too long for
+    // two whole-row stages)
+    if (c->deck.precision == 64 && c->nx >= 256)
+        for (int nseg : {2, 3, 4})
+            for (int st : {2, 3, 4}) {
+                const int seg = segment_for(c->nx, nseg);
+                if (tma_configure(c, 1, st, cons0, 0, seg)) continue;
+                double ms;
+                if ((rc = time_choice(c, steps, &ms))) return rc;
+                ++ncand;
+                if (ms < best_ms) best_ms = ms, best = save_choice(c), bk = 1, bs = st, bseg = seg;
+            }
     if (bk > 0)
         for (int cons = 64; cons <= 352 && cons <= (c->nx + 31) / 32 * 32 + 32; cons += 32) {
-            if (cons == cons0 || tma_configure(c, bk, bs, cons, 0)) continue;
+            if (cons == cons0 || tma_configure(c, bk, bs, cons, 0, bseg)) continue;
             double ms;
             if ((rc = time_choice(c, steps, &ms))) return rc;
             ++ncand;
@@ -1242,6 +1278,7 @@ struct dnslbm_batch {
     // the persistent kernel (default): one cooperative launch per chunk of
     // steps, blocks taking items of work from a per-step counter
     int persistent = 1;
+    int any_q = 0;                      // some channel runs with a constant flow rate
     int pgrid = 0;                      // its blocks (all resident)
     size_t pstage = 0, psmem = 0;       // bytes of one stage, dynamic shared memory
     std::vector<BatchItem> items;       // the items of one step, largest first
@@ -1436,7 +1473,10 @@ static int persist_configure(dnslbm_batch *b)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
     const size_t cap = (size_t)maxsmem - kStaticSmemReserve;
     if (smem > cap || nsm < 1) return -1;
-    const int occ = persist_prepare(b->precision, cap) ? 0 : persist_occupancy_of(b->precision, b->threads, smem);
+    b->any_q = 0;
+    for (auto *c : b->ch) b->any_q |= c->deck.force_mode == DNSLBM_FORCE_CONST_Q;
+    const int occ =
+        persist_prepare(b->precision, cap) ? 0 : persist_occupancy_of(b->precision, b->threads, smem, b->any_q != 0);
     cudaGetLastError();
     if (occ < 1) return -1;
     b->pstage = stage;
@@ -1480,7 +1520,8 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
     for (size_t i = 0; i < b->ch.size(); ++i) {
         dnslbm_ctx *c = b->ch[i];
         const int row_bytes = c->pitch * (int)c->esize;
-        c->tma = TmaArgs{0, 1, stages, row_bytes, ks[i], (c->ny + ks[i] - 1) / ks[i], nullptr};
+        c->tma = TmaArgs{0, 1, stages, row_bytes, ks[i], (c->ny + ks[i] - 1) / ks[i], nullptr, 1, c->nx,
+                         ks[i] * c->pitch};
         c->tma_threads = threads;
         c->tma_smem = smem;
         c->tma_target = occ * nsm;
@@ -1608,7 +1649,7 @@ static int persist_launch(dnslbm_batch *b, int n, int odd)
     a.withhold = b->withhold;
     BCK(cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned) * n, b->stream));
     BCK(cudaMemsetAsync(b->d_arrivals, 0, sizeof(unsigned), b->stream));
-    BCK(launch_persist_batch(b->precision, a, b->pgrid, b->threads, b->psmem, b->stream));
+    BCK(launch_persist_batch(b->precision, a, b->pgrid, b->threads, b->psmem, b->any_q != 0, b->stream));
     return DNSLBM_OK;
 }
 

@@ -65,21 +65,27 @@ __device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b)
 __device__ __forceinline__ float vneg(float a) { return -a; }
 __device__ __forceinline__ float vdiv_fast(float a, float b) { return __fdividef(a, b); }
 
+// The packed add, sub and mul are written in PTX: a product feeding a sum
+// must stay two roundings (the compiler may otherwise fuse the packed
+// intrinsics __fmul2_rn + __fadd2_rn into one fma, which the one-cell form,
+// with __fmul_rn / __fadd_rn, never does).
+#define DNSLBM_F32X2_OP(NAME, OP)                                                     \
+    __device__ __forceinline__ float2 NAME(float2 a, float2 b)                        \
+    {                                                                                 \
+        float2 d;                                                                     \
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\t"                                      \
+            "mov.b64 ra, {%2, %3};\n\t"                                             \
+            "mov.b64 rb, {%4, %5};\n\t" OP " rd, ra, rb;\n\t"                     \
+            "mov.b64 {%0, %1}, rd;\n\t}"                                            \
+            : "=f"(d.x), "=f"(d.y)                                                    \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                \
+        return d;                                                                     \
+    }
+DNSLBM_F32X2_OP(vadd, "add.rn.f32x2")
+DNSLBM_F32X2_OP(vsub, "sub.rn.f32x2")
+DNSLBM_F32X2_OP(vmul, "mul.rn.f32x2")
+#undef DNSLBM_F32X2_OP
 __device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 vsub(float2 a, float2 b)
-{
-    float2 d;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
-        "mov.b64 ra, {%2, %3};\n\t"
-        "mov.b64 rb, {%4, %5};\n\t"
-        "sub.rn.f32x2 rd, ra, rb;\n\t"
-        "mov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(d.x), "=f"(d.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return d;
-}
 __device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float2 vdiv_fast(float2 a, float2 b)
 {
@@ -174,9 +180,15 @@ __device__ __forceinline__ void lp_pair(V (&r)[Q], const LpParams &k, V dr, V Sr
     r[b] = vfma(om1, r[b], vsub(A, B));
 }
 
-// In place on raw values r[19] of one storage type with scale S.
-template <typename T, typename V>
-__device__ __forceinline__ LpCellV<V> lp_collide_v(V (&r)[Q], const LpParams &k)
+// In place on raw values r[19] of one storage type with scale S.  emit(a)
+// is called as soon as r[a] holds its post-collision value (so a caller can
+// store it and free its registers early).
+struct LpNoEmit {
+    __device__ __forceinline__ void operator()(int) const {}
+};
+
+template <typename T, typename V, typename Emit = LpNoEmit>
+__device__ __forceinline__ LpCellV<V> lp_collide_v(V (&r)[Q], const LpParams &k, Emit &&emit = Emit())
 {
     constexpr float S = LpStore<T>::kScale, iS = LpStore<T>::kInv;
     V sum[9], dif[9];
@@ -230,15 +242,14 @@ __device__ __forceinline__ LpCellV<V> lp_collide_v(V (&r)[Q], const LpParams &k)
     r[0] = vfma(vsplat<V>(k.om1), r[0],
                 vmul(vsplat<V>(1.f / 3.f), vfma(vsplat<V>(k.omega), vfma(Srho, nusq15, dr),
                                                 vmul(vsplat<V>(k.m3sg), c.u0))));
-    lp_pair<0>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<1>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<2>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<3>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<4>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<5>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<6>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<7>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
-    lp_pair<8>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);
+    emit(0);
+#define DNSLBM_PAIR(K)                                                 \
+    lp_pair<K>(r, k, dr, Srho, nusq15, a0, beu, c.u0, c.u1, c.u2);     \
+    emit(pair_dir(K));                                                 \
+    emit(lat_opp(pair_dir(K)));
+    DNSLBM_PAIR(0) DNSLBM_PAIR(1) DNSLBM_PAIR(2) DNSLBM_PAIR(3) DNSLBM_PAIR(4)
+    DNSLBM_PAIR(5) DNSLBM_PAIR(6) DNSLBM_PAIR(7) DNSLBM_PAIR(8)
+#undef DNSLBM_PAIR
     return c;
 }
 

@@ -55,12 +55,27 @@ struct PersistArgs {
     int withhold;                  // test switch (0 otherwise): block 0 withholds its first load
 };
 
-// Shared memory after the stages: full[S], empty[S] (8 bytes each) and the
-// stage headers hdr[S][2] (item, row group within the item; item -1 ends
-// the step, row group -1 marks a kind-1 item).
+// Per-stage header, written by the producer before it arms the stage: the
+// channel's arguments and everything the consumers need for the stage's
+// work, so they read no global memory to find it.
+struct StageHeader {
+    ChannelLaunch L;  // the item's channel (copied when the stage held another)
+    BatchItem it;
+    int item;         // index of the item; -1 ends the step
+    int group;        // row group within the item; -1 for a kind-1 item
+    int z, y0;        // plane and first row of the group (kind 1: plane, unused)
+    int chan;         // channel whose arguments L holds
+    int pad_;
+    long long step;   // the channel's step counter
+    double G;         // the force of this step
+    double sh[3];     // the plane's shift (previous plane means)
+};
+
+// Shared memory after the stages: full[S], empty[S] (8 bytes each), then
+// the stage headers.
 __host__ __device__ constexpr size_t persist_smem(int stages, size_t stage_bytes)
 {
-    return (size_t)stages * stage_bytes + 16 * (size_t)stages + 8 * (size_t)stages;
+    return (size_t)stages * stage_bytes + 16 * (size_t)stages + sizeof(StageHeader) * (size_t)stages;
 }
 
 // OR of v over the first nthreads threads (named barrier 2): every one of
@@ -89,7 +104,8 @@ __device__ __forceinline__ void persist_raise(const PersistArgs &a, volatile int
 
 template <typename T, bool ODD>
 __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, int lane, unsigned char *smem,
-                                                 uint64_t *full, uint64_t *empty, int *hdr, volatile int *s_abort)
+                                                 uint64_t *full, uint64_t *empty, StageHeader *hdr,
+                                                 volatile int *s_abort)
 {
     const int S = a.stages;
     int i = 0;            // stage sequence number within the step
@@ -103,17 +119,14 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
         const int st = seq % S;
         if (!*s_abort && !mbar_wait_bounded(empty + st, (uint32_t)((seq / S) & 1), a.wait_ns, s_abort))
             persist_raise(a, s_abort);
-        const int h = hdr[2 * st], g = hdr[2 * st + 1];
-        if (*s_abort || h < 0 || g < 0 || lane >= Q) return;
-        const BatchItem it = a.items[h];
-        const ChannelLaunch &L = a.chans[it.chan];
-        int z, y0;
-        group_origin(L.t, it.first + g, z, y0);
-        const int k = min(L.t.k, L.p.ny - y0);
-        const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
-        const GroupRows gr = L.textured ? group_rows<ODD, 1>(L.p, lane, y0, z, wall)
-                                        : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
-        const size_t dir_bytes = (size_t)L.t.k * L.t.row_bytes;
+        const StageHeader &H = hdr[st];
+        if (*s_abort || H.item < 0 || H.group < 0 || lane >= Q) return;
+        const ChannelLaunch &L = H.L;
+        const int k = min(L.t.k, L.p.ny - H.y0);
+        const int wall = H.z == 0 ? -1 : (H.z == L.p.nz - 1 ? 1 : 0);
+        const GroupRows gr = L.textured ? group_rows<ODD, 1>(L.p, lane, H.y0, H.z, wall)
+                                        : group_rows<ODD, 0>(L.p, lane, H.y0, H.z, wall);
+        const size_t dir_bytes = (size_t)L.t.dir_elems * sizeof(T);
         if (gr.bulk) copy_group<T>(L.p, L.t, gr, k, smem + (size_t)st * a.stage_bytes + lane * dir_bytes, false, nullptr);
         bulk_commit();
     };
@@ -124,56 +137,80 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
         __syncwarp();
         return i % S;
     };
-    for (;;) {
-        int h = 0;
-        if (lane == 0) h = *s_abort ? a.nitems : (int)atomicAdd(a.counters + s, 1u);
-        h = __shfl_sync(0xffffffffu, h, 0);
-        if (h >= a.nitems) break;
+    // the header of a stage: the channel's arguments (when the stage held
+    // another channel) and the item's per-step values
+    auto fill = [&](int st, int h, const BatchItem &it, int g, int z, int y0) {
+        StageHeader &H = hdr[st];
+        const int had = __shfl_sync(0xffffffffu, lane == 0 ? H.chan : 0, 0);
+        if (had != it.chan) {
+            const int *src = reinterpret_cast<const int *>(a.chans + it.chan);
+            int *dst = reinterpret_cast<int *>(&H.L);
+            for (int w = lane; w < (int)(sizeof(ChannelLaunch) / sizeof(int)); w += 32) dst[w] = __ldg(src + w);
+        }
+        if (lane == 0) {
+            const StepArgs &p = a.chans[it.chan].p;
+            H.it = it;
+            H.item = h;
+            H.group = g;
+            H.z = z;
+            H.y0 = y0;
+            H.chan = it.chan;
+            H.step = __ldcg(p.step_ctr);
+            H.G = p.const_q ? __ldcg(p.force + (H.step & 1)) : p.gx;
+            const double *shp = p.shift + (size_t)(H.step & 1) * p.nz * 3 + z * 3;
+            H.sh[0] = __ldcg(shp);
+            H.sh[1] = __ldcg(shp + 1);
+            H.sh[2] = __ldcg(shp + 2);
+        }
+        __syncwarp();
+    };
+    auto take = [&]() { return lane == 0 ? (*s_abort ? a.nitems : (int)atomicAdd(a.counters + s, 1u)) : 0; };
+    int h = __shfl_sync(0xffffffffu, take(), 0);
+    while (h < a.nitems) {
         const BatchItem it = a.items[h];
-        if (it.kind == 1) {  // no copies: the consumers work from global memory
+        const int hn = take();  // the next item, fetched while this one is issued
+        if (it.kind == 1) {     // no copies: the consumers work from global memory
             const int st = next_stage();
-            if (lane == 0) {
-                hdr[2 * st] = h;
-                hdr[2 * st + 1] = -1;
-                mbar_arrive(full + st);
-            }
+            fill(st, h, it, -1, it.plane, it.y0);
+            if (lane == 0) mbar_arrive(full + st);
             __syncwarp();
             ++i;
-            continue;
-        }
-        const ChannelLaunch &L = a.chans[it.chan];
-        const size_t dir_bytes = (size_t)L.t.k * L.t.row_bytes;
-        for (int g = 0; g < it.count; ++g) {
-            const int st = next_stage();
-            int z, y0;
-            group_origin(L.t, it.first + g, z, y0);
-            const int k = min(L.t.k, L.p.ny - y0);
-            const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
-            GroupRows gr{};
-            if (lane < Q)
-                gr = L.textured ? group_rows<ODD, 1>(L.p, lane, y0, z, wall) : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
-            const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && gr.bulk);
-            const bool issue = __shfl_sync(0xffffffffu, *s_abort, 0) == 0 && !withhold;
-            withhold = false;
-            if (issue) {
-                if (lane == 0) {
-                    hdr[2 * st] = h;
-                    hdr[2 * st + 1] = g;
-                    mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * L.t.row_bytes));
+        } else {
+            const ChannelLaunch &L = a.chans[it.chan];
+            const size_t dir_bytes = (size_t)L.t.dir_elems * sizeof(T);
+            for (int g = 0; g < it.count; ++g) {
+                const int st = next_stage();
+                int z, y0;
+                group_origin(L.t, it.first + g, z, y0);
+                const int k = min(L.t.k, L.p.ny - y0);
+                const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
+                GroupRows gr{};
+                if (lane < Q)
+                    gr = L.textured ? group_rows<ODD, 1>(L.p, lane, y0, z, wall)
+                                    : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
+                const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && gr.bulk);
+                const bool issue = __shfl_sync(0xffffffffu, *s_abort, 0) == 0 && !withhold;
+                withhold = false;
+                if (issue) {
+                    fill(st, h, it, g, z, y0);
+                    if (lane == 0) mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * L.t.row_bytes));
+                    __syncwarp();
+                    if (lane < Q && gr.bulk)
+                        copy_group<T>(L.p, L.t, gr, k, smem + (size_t)st * a.stage_bytes + lane * dir_bytes, true,
+                                      full + st);
+                    loaded |= 1u << st;
+                    phase = (phase & ~(1u << st)) | ((unsigned)((i / S) & 1) << st);
                 }
-                __syncwarp();
-                if (lane < Q && gr.bulk)
-                    copy_group<T>(L.p, L.t, gr, k, smem + (size_t)st * a.stage_bytes + lane * dir_bytes, true, full + st);
-                loaded |= 1u << st;
-                phase = (phase & ~(1u << st)) | ((unsigned)((i / S) & 1) << st);
+                ++i;
             }
-            ++i;
         }
+        h = __shfl_sync(0xffffffffu, hn, 0);
+        if (__shfl_sync(0xffffffffu, *s_abort, 0)) break;
     }
     {  // end of the step
         const int st = next_stage();
         if (lane == 0) {
-            hdr[2 * st] = -1;
+            hdr[st].item = -1;
             mbar_arrive(full + st);
         }
         __syncwarp();
@@ -208,9 +245,10 @@ __device__ __forceinline__ void persist_links(const StepArgs &p, const BatchItem
     }
 }
 
-template <typename T, bool ODD>
+template <typename T, bool ODD, bool ANYQ>
 __device__ __forceinline__ void persist_consumers(const PersistArgs &a, unsigned char *smem, uint64_t *full,
-                                                  uint64_t *empty, const int *hdr, int nc, volatile int *s_abort)
+                                                  uint64_t *empty, const StageHeader *hdr, int nc,
+                                                  volatile int *s_abort)
 {
     using LpT = typename std::conditional<std::is_same<T, double>::value, float, T>::type;
     const int S = a.stages;
@@ -225,63 +263,58 @@ __device__ __forceinline__ void persist_consumers(const PersistArgs &a, unsigned
             if (threadIdx.x == 0) persist_raise(a, s_abort);
             return;
         }
-        const int h = hdr[2 * st], g = hdr[2 * st + 1];
-        if (h < 0) return;  // end of the step (the same header for every consumer)
-        const BatchItem it = a.items[h];
-        const ChannelLaunch &L = a.chans[it.chan];
-        const StepArgs &p = L.p;
-        const bool q = p.const_q != 0;
-        const long long step = __ldcg(p.step_ctr);
-        const double G = q ? __ldcg(p.force + (step & 1)) : p.gx;
-        int z, y0 = 0;
-        if (it.kind == 1) z = it.plane;
-        else group_origin(L.t, it.first + g, z, y0);
-        const double *shp = p.shift + (size_t)(step & 1) * p.nz * 3 + z * 3;
-        const double sh[3] = {__ldcg(shp), __ldcg(shp + 1), __ldcg(shp + 2)};
-        if (it.kind == 1) {
-            if (q) persist_links<T, ODD, true>(p, it, G, sh, acc, nc);
-            else persist_links<T, ODD, false>(p, it, G, sh, acc, nc);
+        const StageHeader &H = hdr[st];
+        if (H.item < 0) return;  // end of the step (the same header for every consumer)
+        const StepArgs &p = H.L.p;
+        const bool q = ANYQ && p.const_q != 0;  // a batch without constant-Q channels compiles no such path
+        const double G = H.G;
+        const int z = H.z;
+        if (H.group < 0) {
+            if (q) persist_links<T, ODD, true>(p, H.it, G, H.sh, acc, nc);
+            else persist_links<T, ODD, false>(p, H.it, G, H.sh, acc, nc);
         } else {
-            const int k = min(L.t.k, p.ny - y0);
-            const int dstride = L.t.k * p.pitch;
+            const int k = min(H.L.t.k, p.ny - H.y0);
+            const int dstride = H.L.t.dir_elems;
             T *sb = reinterpret_cast<T *>(smem + (size_t)st * a.stage_bytes);
             [[maybe_unused]] const LpParams lk = lp_params<LpT>((float)p.omega, (float)G);
             if (q) {
-                if (L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
-                else consume_group<T, ODD, true, false>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
+                if (H.L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
+                else consume_group<T, ODD, true, false>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
             } else {
-                if (L.textured) consume_group<T, ODD, false, true>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
-                else consume_group<T, ODD, false, false>(p, lk, sb, dstride, y0, k, z, G, sh, acc, nc);
+                if (H.L.textured) consume_group<T, ODD, false, true>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
+                else consume_group<T, ODD, false, false>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
             }
             fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         }
-        __syncwarp();
-        if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);
-        if (it.kind == 1 || g == it.count - 1) {  // the item is done: its plane contribution
-            plane_contribute(p, acc, z, it.slot, it.ncontrib, step, G, 0, nc);
+        const bool done = H.group < 0 || H.group == H.it.count - 1;
+        if (done) {  // the item is done: its plane contribution (the stage is released after it)
+            plane_contribute(p, acc, z, H.it.slot, H.it.ncontrib, H.step, G, 0, nc);
 #pragma unroll
             for (int r = 0; r < NP; ++r) acc[r] = 0.0;
         }
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);
     }
 }
 
-template <typename T, bool ODD>
+template <typename T, bool ODD, bool ANYQ>
 __device__ __forceinline__ void persist_step(const PersistArgs &a, int s, unsigned char *smem, volatile int *s_abort)
 {
     const int S = a.stages, nc = blockDim.x - 32;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)S * a.stage_bytes);
     uint64_t *empty = full + S;
-    int *hdr = reinterpret_cast<int *>(empty + S);
+    StageHeader *hdr = reinterpret_cast<StageHeader *>(empty + S);
     if (threadIdx.x == 0) {
         for (int st = 0; st < S; ++st) {
             mbar_init(full + st, 1);
             mbar_init(empty + st, nc / 32);
+            hdr[st].chan = -1;  // no channel arguments copied yet
         }
         fence_mbar_init();
     }
     __syncthreads();
     if (threadIdx.x >= nc) persist_producer<T, ODD>(a, s, threadIdx.x - nc, smem, full, empty, hdr, s_abort);
-    else persist_consumers<T, ODD>(a, smem, full, empty, hdr, nc, s_abort);
+    else persist_consumers<T, ODD, ANYQ>(a, smem, full, empty, hdr, nc, s_abort);
 }
 
 // Grid-wide barrier between steps (all blocks are resident: cooperative
@@ -314,15 +347,18 @@ __device__ __forceinline__ bool persist_grid_barrier(const PersistArgs &a, unsig
     return s_go != 0;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kTmaMaxThreads, 1) persist_batch_kernel(const PersistArgs a)
+// ANYQ: some channel runs with a constant flow rate (the launch bounds of
+// TmaBounds follow it).
+template <typename T, bool ANYQ>
+__global__ void __launch_bounds__(TmaBounds<T, ANYQ>::threads, TmaBounds<T, ANYQ>::blocks)
+    persist_batch_kernel(const PersistArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int s_abort;
     for (int s = 0; s < a.nsteps; ++s) {
         if (threadIdx.x == 0) s_abort = 0;
-        if ((a.first_odd + s) & 1) persist_step<T, true>(a, s, smem, &s_abort);
-        else persist_step<T, false>(a, s, smem, &s_abort);
+        if ((a.first_odd + s) & 1) persist_step<T, true, ANYQ>(a, s, smem, &s_abort);
+        else persist_step<T, false, ANYQ>(a, s, smem, &s_abort);
         if (!persist_grid_barrier(a, (unsigned)(s + 1) * gridDim.x)) break;
     }
 }
@@ -330,25 +366,28 @@ __global__ void __launch_bounds__(kTmaMaxThreads, 1) persist_batch_kernel(const 
 template <typename T>
 int persist_set_smem_attr(size_t bytes)
 {
-    return cudaFuncSetAttribute(persist_batch_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
-                   cudaSuccess
-               ? 0
-               : -1;
+    const bool ok = cudaFuncSetAttribute(persist_batch_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes) == cudaSuccess &&
+                    cudaFuncSetAttribute(persist_batch_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes) == cudaSuccess;
+    return ok ? 0 : -1;
 }
 
 template <typename T>
-int persist_occupancy(int threads, size_t smem)
+int persist_occupancy(int threads, size_t smem, bool any_q)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persist_batch_kernel<T>, threads, smem) != cudaSuccess)
-        return 0;
-    return n;
+    if (threads > (any_q ? TmaBounds<T, true>::threads : TmaBounds<T, false>::threads)) return 0;
+    const cudaError_t e =
+        any_q ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persist_batch_kernel<T, true>, threads, smem)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persist_batch_kernel<T, false>, threads, smem);
+    return e == cudaSuccess ? n : 0;
 }
 
 // Cooperative launch: fails (instead of deadlocking) when the grid cannot
 // be resident at once.
 template <typename T>
-cudaError_t launch_persist(const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s)
+cudaError_t launch_persist(const PersistArgs &a, int grid, int threads, size_t smem, bool any_q, cudaStream_t s)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -360,7 +399,8 @@ cudaError_t launch_persist(const PersistArgs &a, int grid, int threads, size_t s
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, persist_batch_kernel<T>, a);
+    return any_q ? cudaLaunchKernelEx(&cfg, persist_batch_kernel<T, true>, a)
+                 : cudaLaunchKernelEx(&cfg, persist_batch_kernel<T, false>, a);
 }
 
 }  // namespace dnslbm

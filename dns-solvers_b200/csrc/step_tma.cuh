@@ -53,8 +53,12 @@ struct TmaArgs {
     int stages;           // row groups in flight per block
     int row_bytes;        // pitch * sizeof(storage)
     int k;                // cell rows per group (consecutive y of one plane)
-    int gpp;              // groups per plane, ceil(ny / k)
+    int gpp;              // groups per plane, ceil(ny / k) * nseg
     const int *planes;    // planes of the kernel's groups in order (nullptr: 0 .. nz-1)
+    // x-segments (FP64 rows too long for two whole-row stages): a group is
+    // one x-segment [s*seg, min((s+1)*seg, nx)) of one row (k = 1), seg even
+    int nseg, seg;
+    int dir_elems;        // elements between two directions' blocks of a stage
 };
 
 // Plane and first row of row group gi.
@@ -62,7 +66,15 @@ __device__ __forceinline__ void group_origin(const TmaArgs &t, int gi, int &z, i
 {
     const int pi = gi / t.gpp;
     z = t.planes ? t.planes[pi] : pi;
-    y0 = (gi - pi * t.gpp) * t.k;
+    y0 = ((gi - pi * t.gpp) / t.nseg) * t.k;
+}
+
+// x-range of row group gi.
+__device__ __forceinline__ void group_xrange(const TmaArgs &t, int gi, int nx, int &x0, int &x1)
+{
+    const int s = (gi % t.gpp) % t.nseg;
+    x0 = s * t.seg;
+    x1 = t.nseg > 1 ? min(x0 + t.seg, nx) : nx;
 }
 
 // ------------------------------------------------------------------ PTX
@@ -189,19 +201,53 @@ __device__ __forceinline__ void copy_group(const StepArgs &p, const TmaArgs &t, 
     }
 }
 
+// The bulk copies of one direction of an x-segment group [x0, x1) (k = 1).
+// Shared memory holds element x of the row at index x - x0 + 2 (a halo of
+// two elements on either side keeps every copy 16-byte aligned).  The load
+// brings [x0, x0 + Lp), Lp = L rounded up to even (the row padding covers
+// the last segment's odd end).  A direction shifted by e_x = +1 in an odd
+// step writes elements x0+1 .. x1; a 16-byte aligned store can start at
+// x0+2 and covers E = (L-1) rounded down to even elements; shifted by -1 it
+// writes x0-1 .. x1-2 and the store covers [x0, x0+E).  The elements outside
+// (at most two per segment and direction) are written by their cells
+// directly (tma_group, SEG).
+template <typename T>
+__device__ __forceinline__ void copy_segment(const StepArgs &p, const GroupRows &g, int x0, int x1, int shift,
+                                             unsigned char *sdir, bool to_smem, uint64_t *bar)
+{
+    const int ny = p.ny, L = x1 - x0, Lp = (L + 1) & ~1;
+    int y = g.y_first;
+    y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
+    T *row = static_cast<T *>(p.pop[g.slot]) + (size_t)(g.zz * ny + y) * p.pitch;
+    if (to_smem) {
+        bulk_g2s(sdir + 2 * sizeof(T), row + x0, (uint32_t)(Lp * sizeof(T)), bar);
+        return;
+    }
+    const int E = (L - 1) & ~1;
+    const int start = shift > 0 ? x0 + 2 : x0, cnt = shift != 0 ? E : Lp;
+    if (cnt > 0) bulk_s2g(row + start, sdir + (size_t)(start - x0 + 2) * sizeof(T), (uint32_t)(cnt * sizeof(T)));
+}
+
 // ------------------------------------------------------------------ cells
 // The k cell rows of a row group from the stage buffer: direction A's
 // element x of row j at sb[A * dstride + j * pitch + x].  The group's k * nx
 // cells are spread over the nc consumer threads as one range, so rows
 // shorter than the consumer set keep every thread busy.
 // WALL: 0 interior plane, -1 bottom plane, +1 top plane.
-template <typename T, bool ODD, bool CONSTQ, bool TEXTURED, int WALL>
+// SEG: the group is the x-segment [x0, x1) of one row (k = 1), element x at
+// shared-memory index x - x0 + 2; the segment's two edge cells move their
+// e_x-shifted directions of an odd step through global memory (the element
+// may lie outside the segment's copies), and into shared memory too where
+// the segment's bulk store will write it.
+template <typename T, bool ODD, bool CONSTQ, bool TEXTURED, int WALL, bool SEG = false>
 __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride, int y0, int k, int z, double G,
-                                          const double *shift, double (&acc)[NP], int nc)
+                                          const double *shift, double (&acc)[NP], int nc, int x0 = 0, int x1 = -1)
 {
     using V = RegT<T>;
     const double c0 = shift[0], c1 = shift[1], c2 = shift[2];
     const int nx = p.nx, pitch = p.pitch;
+    if (!SEG) x0 = 0, x1 = nx;
+    const int sxoff = SEG ? 2 - x0 : 0;  // shared-memory index of element x: x + sxoff
     // low precision: a row's few cells per thread are summed in FP32, then
     // added to the FP64 accumulators when the thread moves to another row
     float racc[NP];
@@ -210,8 +256,15 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
     // one cell (row j of the group, column x)
     auto cell = [&](int j, int x) {
         const int y = y0 + j;
-        T *sbj = sb + (size_t)j * pitch;
+        T *sbj = sb + (size_t)j * pitch + sxoff;
         const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+        const bool edge = SEG && ODD && (x == x0 || x == x1 - 1);
+        // global element of an e_x-shifted direction A of an odd step (edge cells)
+        auto shifted_ptr = [&](int A, int xs) {
+            int yy = y + lat_ey(A);
+            yy = yy < 0 ? yy + p.ny : (yy >= p.ny ? yy - p.ny : yy);
+            return static_cast<T *>(p.pop[A]) + ((size_t)(z + lat_ez(A)) * p.ny + yy) * pitch + xs;
+        };
         unsigned bits = 0x1fu;
         if (TEXTURED && WALL != 0) bits = p.wallmask[(size_t)(WALL > 0) * nx * p.ny + (size_t)y * nx + x];
         Nbr n;
@@ -233,7 +286,8 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
                 v = ld_glb<T>(static_cast<const T *>(p.pop[slot]) + idx);
             } else {
                 const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
-                v = ld_raw<T>(sbj + A * dstride + xs);
+                if (SEG && edge && !wdir && lat_ex(A) != 0) v = ld_glb<T>(shifted_ptr(A, xs));
+                else v = ld_raw<T>(sbj + A * dstride + xs);
             }
             f[ODD ? lat_opp(A) : A] = v;
         }
@@ -308,7 +362,12 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
                 st_raw<T>(static_cast<T *>(p.pop[slot]) + idx, v);
             } else {
                 const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
-                st_raw<T>(sbj + A * dstride + xs, v);
+                if (SEG && edge && !wdir && lat_ex(A) != 0) {
+                    st_raw<T>(shifted_ptr(A, xs), v);
+                    if ((unsigned)(xs + sxoff) < (unsigned)dstride) st_raw<T>(sbj + A * dstride + xs, v);
+                } else {
+                    st_raw<T>(sbj + A * dstride + xs, v);
+                }
             }
         }
     };
@@ -318,6 +377,11 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
             for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i], racc[i] = 0.f;
         }
     };
+    if (SEG) {
+        for (int x = x0 + threadIdx.x; x < x1; x += nc) cell(0, x);
+        flush();
+        return;
+    }
     if (nx >= nc) {  // rows at least as long as the consumer set: row by row
         for (int j = 0; j < k; ++j) {
             for (int x = threadIdx.x; x < nx; x += nc) cell(j, x);
@@ -406,20 +470,31 @@ __device__ __forceinline__ void tma_group2(const StepArgs &p, const LpParams &lk
             else v = make_float2(IO::ld1(row + xm0), IO::ld1(row + x));
             f[ODD ? lat_opp(A) : A] = v;
         }
+        // the post-collision value of population a goes to direction A = a
+        // (odd step) or opp(a) (even step) at once, with the writer-side sums
         float2 s = make_float2(0.f, 0.f), m = make_float2(0.f, 0.f);
-        const LpCellV<float2> c = lp_collide_v<T, float2>(f, lk);
-        if (CONSTQ) {  // writer side: sums of the post-collision values
-            s = f[0];
-#pragma unroll
-            for (int a = 1; a < Q; ++a) s = vadd(s, f[a]);
-            bool first = true;
-#pragma unroll
-            for (int a = 0; a < Q; ++a) {
-                if (!lat_ex(a)) continue;
-                if (first) m = lat_ex(a) > 0 ? f[a] : vneg(f[a]);
-                else m = lat_ex(a) > 0 ? vadd(m, f[a]) : vsub(m, f[a]);
-                first = false;
+        auto emit = [&](int a) {
+            const int A = ODD ? a : lat_opp(a);
+            const bool wdir = ODD && lat_ez(A) != 0 && lat_ez(A) == WALL;
+            T *row = sbj + A * dstride;
+            const float2 v = f[a];
+            if (!ODD || wdir || lat_ex(A) == 0) {
+                IO::st2(row + x, v);  // for a one-cell pair the second lane lands in the row padding
+            } else if (lat_ex(A) > 0) {
+                IO::st1(row + xp0, v.x);
+                if (two) IO::st1(row + xp1, v.y);
+            } else {
+                IO::st1(row + xm0, v.x);
+                if (two) IO::st1(row + x, v.y);
             }
+            if (CONSTQ) {
+                s = vadd(s, v);
+                if (lat_ex(a) > 0) m = vadd(m, v);
+                if (lat_ex(a) < 0) m = vsub(m, v);
+            }
+        };
+        const LpCellV<float2> c = lp_collide_v<T, float2>(f, lk, emit);
+        if (CONSTQ) {
             s = vmul(s, vsplat<float2>(iS));
             m = vmul(m, vsplat<float2>(iS));
             if (WALL != 0) {  // smooth walls: every link into the wall bounces back, -2 e_x (w + d)
@@ -454,21 +529,6 @@ __device__ __forceinline__ void tma_group2(const StepArgs &p, const LpParams &lk
             if (CONSTQ) {
                 racc[6].x += s.x;
                 racc[7].x += m.x;
-            }
-        }
-#pragma unroll
-        for (int A = 0; A < Q; ++A) {
-            const bool wdir = ODD && lat_ez(A) != 0 && lat_ez(A) == WALL;
-            T *row = sbj + A * dstride;
-            const float2 v = f[ODD ? A : lat_opp(A)];
-            if (!ODD || wdir || lat_ex(A) == 0) {
-                IO::st2(row + x, v);  // for a one-cell pair the second lane lands in the row padding
-            } else if (lat_ex(A) > 0) {
-                IO::st1(row + xp0, v.x);
-                if (two) IO::st1(row + xp1, v.y);
-            } else {
-                IO::st1(row + xm0, v.x);
-                if (two) IO::st1(row + x, v.y);
             }
         }
     };
@@ -512,8 +572,13 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
                                              unsigned char *smem, uint64_t *full, uint64_t *empty, volatile int *abort)
 {
     const int S = t.stages;
-    const size_t dir_bytes = (size_t)t.k * t.row_bytes, stage_bytes = (size_t)Q * dir_bytes;
+    const size_t dir_bytes = (size_t)t.dir_elems * sizeof(T), stage_bytes = (size_t)Q * dir_bytes;
     const bool withhold = p.withhold_stage != 0 && g0 == 0;
+    // e_x shift of direction `lane`'s elements in an odd step (0: the cell's own column)
+    auto shift_of = [&](int wall) {
+        const int ez = lat_ez(lane < Q ? lane : 0);
+        return (ODD && !(ez != 0 && ez == wall) && lane < Q) ? lat_ex(lane) : 0;
+    };
     unsigned loaded = 0;  // bit s: a load into stage s was issued (its phase is the last one armed)
     unsigned phase = 0;   // bit s: parity of that phase
     for (int i = 0; i < n + S; ++i) {
@@ -531,7 +596,15 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
             if (lane < Q && !*abort) {
                 const GroupRows g = group_rows<ODD, TEX>(p, lane, y0, z, wall);
-                if (g.bulk) copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, false, nullptr);
+                if (g.bulk) {
+                    if (t.nseg > 1) {
+                        int x0, x1;
+                        group_xrange(t, gi, p.nx, x0, x1);
+                        copy_segment<T>(p, g, x0, x1, shift_of(wall), stage + (size_t)lane * dir_bytes, false, nullptr);
+                    } else {
+                        copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, false, nullptr);
+                    }
+                }
                 bulk_commit();
             }
         }
@@ -549,9 +622,17 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             // one decision for the whole warp: lane 0's reading of the flag
             const bool issue = __shfl_sync(0xffffffffu, *abort, 0) == 0 && !(withhold && i == 0);
             if (issue) {
-                if (lane == 0) mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * t.row_bytes));
+                int x0 = 0, x1 = p.nx;
+                if (t.nseg > 1) group_xrange(t, gi, p.nx, x0, x1);
+                const size_t bytes = t.nseg > 1 ? (size_t)((x1 - x0 + 1) & ~1) * sizeof(T) : (size_t)k * t.row_bytes;
+                if (lane == 0) mbar_expect_tx(full + st, (uint32_t)(__popc(vote) * bytes));
                 __syncwarp();
-                if (lane < Q && g.bulk) copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, true, full + st);
+                if (lane < Q && g.bulk) {
+                    if (t.nseg > 1)
+                        copy_segment<T>(p, g, x0, x1, shift_of(wall), stage + (size_t)lane * dir_bytes, true, full + st);
+                    else
+                        copy_group<T>(p, t, g, k, stage + (size_t)lane * dir_bytes, true, full + st);
+                }
                 loaded |= 1u << st;
                 phase = (phase & ~(1u << st)) | ((unsigned)((i / S) & 1) << st);
             }
@@ -567,6 +648,18 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
 }
 
 constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer warp
+
+// Launch bounds of the row-pipelined kernels.  The FP32/FP16 constant-force
+// step fits 128 registers without spilling, so it is compiled for up to 256
+// threads and two blocks per SM (more warps in flight to hide the latency of
+// its dependency chains); the FP64 step and the constant-Q steps keep up to
+// 168 registers and 384 threads.
+template <typename T, bool CONSTQ>
+struct TmaBounds {
+    static constexpr bool wide = std::is_same<T, double>::value || CONSTQ;
+    static constexpr int threads = wide ? kTmaMaxThreads : 256;
+    static constexpr int blocks = wide ? 1 : 2;
+};
 
 // The consumers' work on one row group in a stage: FP64 one cell per thread
 // and iteration in the reference's operand order; FP32/FP16 cell pairs on
@@ -603,7 +696,7 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
     const int n = min(g0 + G_, t.ngroups) - g0;
     if (n <= 0) return;  // block-uniform; empty blocks contribute to no plane
     const int nc = blockDim.x - 32;  // consumer threads; the last warp produces
-    const size_t dir_bytes = (size_t)t.k * t.row_bytes, stage_bytes = (size_t)Q * dir_bytes;
+    const size_t dir_bytes = (size_t)t.dir_elems * sizeof(T), stage_bytes = (size_t)Q * dir_bytes;
     uint64_t *full = reinterpret_cast<uint64_t *>(tma_smem + (size_t)S * stage_bytes);
     uint64_t *empty = full + S;
     if (threadIdx.x == 0) {
@@ -623,7 +716,7 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
     const long long step = *p.step_ctr;
     const double G = CONSTQ ? p.force[step & 1] : p.gx;
     const double *shift_now = p.shift + (size_t)(step & 1) * p.nz * 3;
-    const int dstride = t.k * p.pitch;
+    const int dstride = t.dir_elems;
     [[maybe_unused]] const LpParams lk = lp_params<typename std::conditional<std::is_same<T, double>::value, float, T>::type>(
         (float)p.omega, (float)G);
     double acc[NP];
@@ -640,7 +733,22 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
             atomicExch(reinterpret_cast<unsigned long long *>(p.status + 1), 1ull);
         }
         T *sb = reinterpret_cast<T *>(tma_smem + (size_t)st * stage_bytes);
-        consume_group<T, ODD, CONSTQ, TEX != 0>(p, lk, sb, dstride, y0, k, z, G, shift_now + z * 3, acc, nc);
+        if constexpr (std::is_same<T, double>::value) {
+            if (t.nseg > 1) {  // an x-segment of one row
+                int x0, x1;
+                group_xrange(t, gi, p.nx, x0, x1);
+                constexpr bool TXT = TEX != 0;
+                const double *sh = shift_now + z * 3;
+                if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1, true>(p, sb, dstride, y0, 1, z, G, sh, acc, nc, x0, x1);
+                else if (z == p.nz - 1)
+                    tma_group<T, ODD, CONSTQ, TXT, 1, true>(p, sb, dstride, y0, 1, z, G, sh, acc, nc, x0, x1);
+                else tma_group<T, ODD, CONSTQ, TXT, 0, true>(p, sb, dstride, y0, 1, z, G, sh, acc, nc, x0, x1);
+            } else {
+                consume_group<T, ODD, CONSTQ, TEX != 0>(p, lk, sb, dstride, y0, k, z, G, shift_now + z * 3, acc, nc);
+            }
+        } else {
+            consume_group<T, ODD, CONSTQ, TEX != 0>(p, lk, sb, dstride, y0, k, z, G, shift_now + z * 3, acc, nc);
+        }
         fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(empty + st);
@@ -656,7 +764,8 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
 }
 
 template <typename T, bool ODD, bool CONSTQ, int TEX>
-__global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_kernel(const StepArgs p, const TmaArgs t)
+__global__ void __launch_bounds__(TmaBounds<T, CONSTQ>::threads, TmaBounds<T, CONSTQ>::blocks)
+    step_tma_kernel(const StepArgs p, const TmaArgs t)
 {
     extern __shared__ __align__(128) unsigned char tma_smem[];
     tma_step_body<T, ODD, CONSTQ, TEX>(p, t, blockIdx.x, tma_smem);
@@ -716,13 +825,14 @@ int tma_set_smem_attr(size_t bytes)
 }
 
 template <typename T>
-int tma_occupancy(int threads, size_t smem)
+int tma_occupancy(int threads, size_t smem, bool const_q)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0>, threads, smem) !=
-        cudaSuccess)
-        return 0;
-    return n;
+    if (threads > (const_q ? TmaBounds<T, true>::threads : TmaBounds<T, false>::threads)) return 0;
+    const cudaError_t e =
+        const_q ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, true, 0>, threads, smem)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0>, threads, smem);
+    return e == cudaSuccess ? n : 0;
 }
 
 template <typename T>

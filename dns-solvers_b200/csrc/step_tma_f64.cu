@@ -6,7 +6,7 @@
 namespace dnslbm {
 
 int tma_prepare_f64(size_t smem) { return tma_set_smem_attr<double>(smem); }
-int tma_occupancy_f64(int threads, size_t smem) { return tma_occupancy<double>(threads, smem); }
+int tma_occupancy_f64(int threads, size_t smem, bool const_q) { return tma_occupancy<double>(threads, smem, const_q); }
 void launch_tma_f64(const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd, int tex,
                     cudaStream_t s)
 {
@@ -28,10 +28,10 @@ void launch_links_f64(const LinksLaunch *tab, int n, int blocks, bool odd, cudaS
 }
 
 int persist_prepare_f64(size_t smem) { return persist_set_smem_attr<double>(smem); }
-int persist_occupancy_f64(int threads, size_t smem) { return persist_occupancy<double>(threads, smem); }
-cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s)
+int persist_occupancy_f64(int threads, size_t smem, bool any_q) { return persist_occupancy<double>(threads, smem, any_q); }
+cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, bool any_q, cudaStream_t s)
 {
-    return launch_persist<double>(a, grid, threads, smem, s);
+    return launch_persist<double>(a, grid, threads, smem, any_q, s);
 }
 
 }  // namespace dnslbm

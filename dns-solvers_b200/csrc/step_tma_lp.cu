@@ -8,9 +8,9 @@ int tma_prepare_lp(int precision, size_t smem)
 {
     return precision == 32 ? tma_set_smem_attr<float>(smem) : tma_set_smem_attr<__half>(smem);
 }
-int tma_occupancy_lp(int precision, int threads, size_t smem)
+int tma_occupancy_lp(int precision, int threads, size_t smem, bool const_q)
 {
-    return precision == 32 ? tma_occupancy<float>(threads, smem) : tma_occupancy<__half>(threads, smem);
+    return precision == 32 ? tma_occupancy<float>(threads, smem, const_q) : tma_occupancy<__half>(threads, smem, const_q);
 }
 void launch_tma_lp(int precision, const StepArgs &p, const TmaArgs &t, int grid, int threads, size_t smem, bool odd,
                    int tex, cudaStream_t s)
@@ -45,14 +45,16 @@ int persist_prepare_lp(int precision, size_t smem)
 {
     return precision == 32 ? persist_set_smem_attr<float>(smem) : persist_set_smem_attr<__half>(smem);
 }
-int persist_occupancy_lp(int precision, int threads, size_t smem)
+int persist_occupancy_lp(int precision, int threads, size_t smem, bool any_q)
 {
-    return precision == 32 ? persist_occupancy<float>(threads, smem) : persist_occupancy<__half>(threads, smem);
+    return precision == 32 ? persist_occupancy<float>(threads, smem, any_q)
+                           : persist_occupancy<__half>(threads, smem, any_q);
 }
-cudaError_t launch_persist_lp(int precision, const PersistArgs &a, int grid, int threads, size_t smem, cudaStream_t s)
+cudaError_t launch_persist_lp(int precision, const PersistArgs &a, int grid, int threads, size_t smem, bool any_q,
+                              cudaStream_t s)
 {
-    return precision == 32 ? launch_persist<float>(a, grid, threads, smem, s)
-                           : launch_persist<__half>(a, grid, threads, smem, s);
+    return precision == 32 ? launch_persist<float>(a, grid, threads, smem, any_q, s)
+                           : launch_persist<__half>(a, grid, threads, smem, any_q, s);
 }
 
 }  // namespace dnslbm
