@@ -262,7 +262,8 @@ def batched_summary(b):
     return {"channels": b["channels"], "seed": b["seed"], "cells": b["cells"], "dtype": b["dtype"],
             "value": b["value"], "ms_per_step": b["ms_per_step"], "one_at_a_time": b["one_at_a_time"]["value"],
             "speedup_vs_one_at_a_time": b["speedup_vs_one_at_a_time"],
-            "whole_step_frac": b["whole_step_frac_of_hbm"], "kernel": b["kernel_config"].split(":")[0]}
+            "whole_step_frac": b["whole_step_frac_of_hbm"], "kernel": b["kernel_config"].split(":")[0],
+            "one_launch_per_step": b["one_launch_per_step"]["value"]}
 
 
 def timed_run(ch, steps, warmup):
@@ -295,16 +296,27 @@ def batched_report(args, dev):
                          device=dev) for w in chans]
     cells = sum(w.cells for w in chans)
     warm = max(args.warmup, 3)
-    with dnslbm.Batch(decks) as b:
-        for c, fl in zip(b.channels, flags):
-            c.set_flags(fl)
-        tune = None if args.no_autotune else b.autotune(8)
-        for c, w, fl in zip(b.channels, chans, flags):
-            c.load_state(inputs.rest_solids(fields[w.nz], fl) if inputs.needs_general(w) else fields[w.nz])
-        b.step_timed(warm)
-        ms_b = b.step_timed(args.steps)
-        kdesc = b.kernel
-        bpc = b.channels[0].bytes_per_cell
+
+    def run_batch(launch_mode):
+        old = os.environ.pop("DNSLBM_BATCH", None)
+        if launch_mode:
+            os.environ["DNSLBM_BATCH"] = "launch"
+        try:
+            with dnslbm.Batch(decks) as b:
+                for c, fl in zip(b.channels, flags):
+                    c.set_flags(fl)
+                tune = None if args.no_autotune else b.autotune(8)
+                for c, w, fl in zip(b.channels, chans, flags):
+                    c.load_state(inputs.rest_solids(fields[w.nz], fl) if inputs.needs_general(w) else fields[w.nz])
+                b.step_timed(warm)
+                return b.step_timed(args.steps), b.kernel, b.channels[0].bytes_per_cell, tune
+        finally:
+            os.environ.pop("DNSLBM_BATCH", None)
+            if old is not None:
+                os.environ["DNSLBM_BATCH"] = old
+
+    ms_b, kdesc, bpc, tune = run_batch(False)
+    ms_l, kdesc_l, _, _ = run_batch(True)
     ms_alone = 0.0
     for w, fl in zip(chans, flags):
         with dnslbm.Channel(w.nx, w.ny, w.nz, w.omega, ubulk=w.ubulk, gx=w.gx, precision=32, bc_mode=mode(w),
@@ -326,7 +338,9 @@ def batched_report(args, dev):
                               "ms_per_step": round(ms_alone / args.steps, 4)},
             "speedup_vs_one_at_a_time": round(ms_alone / ms_b, 3),
             "whole_step_frac_of_hbm": round(bpc * cells / (ms_b / args.steps / 1e3) / 1e9 / peak, 4),
-            "kernel_config": kdesc}
+            "kernel_config": kdesc, "autotune": tune,
+            "one_launch_per_step": {"value": round(cells * args.steps / (ms_l / 1e3) / 1e6, 1), "unit": "MLUPS",
+                                    "ms_per_step": round(ms_l / args.steps, 4), "kernel_config": kdesc_l}}
 
 
 def run_ours(args):

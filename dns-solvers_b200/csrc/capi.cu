@@ -112,9 +112,13 @@ struct dnslbm_ctx {
     dim3 grid, block;
     int rows = 8;
     int slots = 1;  // partial-sum slots per plane
-    // row-pipelined (bulk-copy) step
+    // row-pipelined (bulk-copy) step; with odd_split the odd steps use their
+    // own launch shape (odd_*), chosen by the autotuner
     int use_tma = 0, tma_threads = 0, tma_grid = 0;
-    char kernel_desc[256] = {0};
+    int odd_split = 0, odd_threads = 0, odd_grid = 0, odd_target = 0;
+    size_t odd_smem = 0;
+    TmaArgs odd_tma{};
+    char kernel_desc[512] = {0};
     size_t tma_smem = 0;
     TmaArgs tma{};
     int have_state = 0;
@@ -226,15 +230,21 @@ constexpr size_t kStaticSmemReserve = 4096;
 
 // Row groups of the row-pipelined kernel over its planes (all planes, or the
 // planes without link masks) shared among tma_target blocks.
+static void tma_layout_of(dnslbm_ctx *c, TmaArgs &t, int target, int &grid)
+{
+    const int ngroups = t.gpp * c->nclean;
+    target = std::max(1, target);
+    const int GB = std::max(1, (ngroups + target - 1) / target);
+    t.ngroups = ngroups;
+    t.groups_per_block = GB;
+    t.planes = c->nclean < c->nz ? c->plane_list : nullptr;
+    grid = (ngroups + GB - 1) / GB;
+}
+
 static void tma_layout(dnslbm_ctx *c)
 {
-    const int ngroups = c->tma.gpp * c->nclean;
-    const int target = std::max(1, c->tma_target);
-    const int GB = std::max(1, (ngroups + target - 1) / target);
-    c->tma.ngroups = ngroups;
-    c->tma.groups_per_block = GB;
-    c->tma.planes = c->nclean < c->nz ? c->plane_list : nullptr;
-    c->tma_grid = (ngroups + GB - 1) / GB;
+    tma_layout_of(c, c->tma, c->tma_target, c->tma_grid);
+    if (c->odd_split) tma_layout_of(c, c->odd_tma, c->odd_target, c->odd_grid);
 }
 
 // seg > 0 (FP64 only): groups are x-segments of seg elements (even) of one
@@ -268,6 +278,7 @@ static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bp
     if (occ < 1) return -1;
     const int gpp = (c->ny + k - 1) / k * nseg;
     c->use_tma = 1;
+    c->odd_split = 0;
     c->tma_threads = threads;
     c->tma_smem = smem;
     c->tma_target = occ * nsm;
@@ -290,6 +301,11 @@ static void describe_kernel(dnslbm_ctx *c)
         if (c->tma.nseg > 1 && m > 0 && m < (int)sizeof c->kernel_desc)
             m += snprintf(c->kernel_desc + m, sizeof c->kernel_desc - m, ", rows in %d x-segments of %d", c->tma.nseg,
                           c->tma.seg);
+        if (c->odd_split && m > 0 && m < (int)sizeof c->kernel_desc)
+            m += snprintf(c->kernel_desc + m, sizeof c->kernel_desc - m,
+                          "; odd steps: %d blocks x %d threads, %d groups of %d rows/block, %d stages, %zu B smem",
+                          c->odd_grid, c->odd_threads, c->odd_tma.groups_per_block, c->odd_tma.k, c->odd_tma.stages,
+                          c->odd_smem);
         if (c->ndirty > 0 && m > 0 && m < (int)sizeof c->kernel_desc)
             snprintf(c->kernel_desc + m, sizeof c->kernel_desc - m, " + links_pass_kernel over %d planes", c->ndirty);
     } else {
@@ -820,12 +836,14 @@ static int launch_steps(dnslbm_ctx *c, long n, bool timed, double *ms_even, doub
                 CK(cudaStreamWaitEvent(c->side, c->fj[0], 0));
             }
             if (c->tma.ngroups > 0) {
+                const bool alt = odd && c->odd_split;
+                const TmaArgs &t = alt ? c->odd_tma : c->tma;
+                const int grid = alt ? c->odd_grid : c->tma_grid, threads = alt ? c->odd_threads : c->tma_threads;
+                const size_t smem = alt ? c->odd_smem : c->tma_smem;
                 if (c->deck.precision == 64)
-                    launch_tma_f64(p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd, c->walls_textured,
-                                   c->stream);
+                    launch_tma_f64(p, t, grid, threads, smem, odd, c->walls_textured, c->stream);
                 else
-                    launch_tma_lp(c->deck.precision, p, c->tma, c->tma_grid, c->tma_threads, c->tma_smem, odd,
-                                  c->walls_textured, c->stream);
+                    launch_tma_lp(c->deck.precision, p, t, grid, threads, smem, odd, c->walls_textured, c->stream);
             }
             if (c->ndirty > 0) {
                 const int blocks = c->ndirty * (int)(c->grid.x * c->grid.y);
@@ -1166,11 +1184,15 @@ struct TmaChoice {
     int use_tma, threads, grid, target;
     size_t smem;
     TmaArgs t;
+    int odd_split, odd_threads, odd_grid, odd_target;
+    size_t odd_smem;
+    TmaArgs odd_t;
 };
 
 static TmaChoice save_choice(const dnslbm_ctx *c)
 {
-    return {c->use_tma, c->tma_threads, c->tma_grid, c->tma_target, c->tma_smem, c->tma};
+    return {c->use_tma,   c->tma_threads, c->tma_grid,   c->tma_target, c->tma_smem, c->tma,
+            c->odd_split, c->odd_threads, c->odd_grid,   c->odd_target, c->odd_smem, c->odd_tma};
 }
 static void load_choice(dnslbm_ctx *c, const TmaChoice &k)
 {
@@ -1180,10 +1202,31 @@ static void load_choice(dnslbm_ctx *c, const TmaChoice &k)
     c->tma_target = k.target;
     c->tma_smem = k.smem;
     c->tma = k.t;
+    c->odd_split = k.odd_split;
+    c->odd_threads = k.odd_threads;
+    c->odd_grid = k.odd_grid;
+    c->odd_target = k.odd_target;
+    c->odd_smem = k.odd_smem;
+    c->odd_tma = k.odd_t;
 }
 
-// device time per step of the current launch shape, on a rest state
-static int time_choice(dnslbm_ctx *c, int steps, double *ms)
+// A choice whose even steps use shape e and odd steps shape o (both whole
+// row-pipelined shapes).
+static TmaChoice split_choice(const TmaChoice &e, const TmaChoice &o)
+{
+    TmaChoice k = e;
+    k.odd_split = 1;
+    k.odd_threads = o.threads;
+    k.odd_grid = o.grid;
+    k.odd_target = o.target;
+    k.odd_smem = o.smem;
+    k.odd_t = o.t;
+    return k;
+}
+
+// device time per even and per odd step of the current launch shape, on a
+// rest state
+static int time_choice(dnslbm_ctx *c, int steps, double *ms, double *ms_even = nullptr, double *ms_odd = nullptr)
 {
     int rc = reset_counters(c);
     if (rc) return rc;
@@ -1196,6 +1239,9 @@ static int time_choice(dnslbm_ctx *c, int steps, double *ms)
     if ((rc = launch_steps(c, steps, true, &e, &o))) return rc;
     if ((rc = check_status(c))) return rc;
     *ms = (e + o) / steps;
+    const int ne = (steps + 1) / 2, no = steps / 2;  // the timed run starts on an even step
+    if (ms_even) *ms_even = ne ? e / ne : 0.0;
+    if (ms_odd) *ms_odd = no ? o / no : 0.0;
     return DNSLBM_OK;
 }
 
@@ -1218,17 +1264,30 @@ extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t re
         if (ms < best_ms) best_ms = ms, best = save_choice(c);
     }
     // row-pipelined: group rows x stages at the default consumer count, then
-    // the consumer count for the best pair
+    // the consumer count and the blocks per SM for the best pair; the even
+    // and the odd steps are timed apart and may end with different shapes
+    // (their address sets differ: one row position, or three planes x three
+    // rows)
     const int cap = c->deck.precision == 64 ? 320 : (c->deck.precision == 32 ? 192 : 128);
     const int cons0 = std::min(cap, (c->nx + 31) / 32 * 32);
-    int bk = -1, bs = -1, bseg = 0;
+    struct Best {
+        double ms = 1e30;
+        TmaChoice ch{};
+        int k = -1, st = -1, seg = 0, cons = 0;
+    } be, bo;  // best even / odd step shape
+    auto timed = [&](int k, int st, int seg, int cons) -> int {
+        double ms, e, o;
+        int r = time_choice(c, steps, &ms, &e, &o);
+        if (r) return r;
+        ++ncand;
+        if (e < be.ms) be.ms = e, be.ch = save_choice(c), be.k = k, be.st = st, be.seg = seg, be.cons = cons;
+        if (o < bo.ms) bo.ms = o, bo.ch = save_choice(c), bo.k = k, bo.st = st, bo.seg = seg, bo.cons = cons;
+        return DNSLBM_OK;
+    };
     for (int k : {1, 2, 4, 8})
         for (int st : {2, 3, 4}) {
             if (k > c->ny || tma_configure(c, k, st, cons0, 0)) continue;
-            double ms;
-            if ((rc = time_choice(c, steps, &ms))) return rc;
-            ++ncand;
-            if (ms < best_ms) best_ms = ms, best = save_choice(c), bk = k, bs = st, bseg = 0;
+            if ((rc = timed(k, st, 0, cons0))) return rc;
         }
     // FP64 rows as x-segments (the only bulk-copy form for rows too long for
     // two whole-row stages)
@@ -1237,19 +1296,34 @@ extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t re
             for (int st : {2, 3, 4}) {
                 const int seg = segment_for(c->nx, nseg);
                 if (tma_configure(c, 1, st, cons0, 0, seg)) continue;
-                double ms;
-                if ((rc = time_choice(c, steps, &ms))) return rc;
-                ++ncand;
-                if (ms < best_ms) best_ms = ms, best = save_choice(c), bk = 1, bs = st, bseg = seg;
+                if ((rc = timed(1, st, seg, cons0))) return rc;
             }
-    if (bk > 0)
+    // consumer counts, then a cap on the blocks per SM, for each parity's best
+    for (int pass = 0; pass < 2; ++pass) {
+        const Best b0 = pass == 0 ? be : bo;
+        if (b0.k < 0 || (pass == 1 && bo.k == be.k && bo.st == be.st && bo.seg == be.seg)) continue;
         for (int cons = 64; cons <= 352 && cons <= (c->nx + 31) / 32 * 32 + 32; cons += 32) {
-            if (cons == cons0 || tma_configure(c, bk, bs, cons, 0, bseg)) continue;
-            double ms;
-            if ((rc = time_choice(c, steps, &ms))) return rc;
-            ++ncand;
-            if (ms < best_ms) best_ms = ms, best = save_choice(c);
+            if (cons == cons0 || tma_configure(c, b0.k, b0.st, cons, 0, b0.seg)) continue;
+            if ((rc = timed(b0.k, b0.st, b0.seg, cons))) return rc;
         }
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+        const Best b0 = pass == 0 ? be : bo;
+        if (b0.k < 0) continue;
+        for (int bps : {1, 2, 3}) {
+            if (tma_configure(c, b0.k, b0.st, b0.cons, bps, b0.seg)) continue;
+            if ((rc = timed(b0.k, b0.st, b0.seg, b0.cons))) return rc;
+        }
+    }
+    if (be.k > 0) {
+        const bool same = be.ch.threads == bo.ch.threads && be.ch.grid == bo.ch.grid && be.ch.smem == bo.ch.smem &&
+                          be.ch.t.k == bo.ch.t.k && be.ch.t.stages == bo.ch.t.stages && be.ch.t.nseg == bo.ch.t.nseg;
+        load_choice(c, same ? be.ch : split_choice(be.ch, bo.ch));
+        double ms;
+        if ((rc = time_choice(c, steps, &ms))) return rc;  // the combination, measured
+        ++ncand;
+        if (ms < best_ms) best_ms = ms, best = save_choice(c);
+    }
     load_choice(c, best);
     describe_kernel(c);
     // leave the context as created: no state, counters clear
@@ -1522,6 +1596,7 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
         const int row_bytes = c->pitch * (int)c->esize;
         c->tma = TmaArgs{0, 1, stages, row_bytes, ks[i], (c->ny + ks[i] - 1) / ks[i], nullptr, 1, c->nx,
                          ks[i] * c->pitch};
+        c->odd_split = 0;
         c->tma_threads = threads;
         c->tma_smem = smem;
         c->tma_target = occ * nsm;

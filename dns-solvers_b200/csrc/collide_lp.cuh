@@ -156,7 +156,8 @@ __device__ __forceinline__ V lp_eu(V u0, V u1, V u2)
 }
 
 // Pair (a, opp a): A = w (omega (dr + S rho t) + S G (9 e_x e.u - 3 u_x)),
-// B = w (3 omega S rho e.u + 3 S G e_x), t = 4.5 (e.u)^2 - 1.5 u.u.
+// B = w (3 omega S rho e.u + 3 S G e_x), t = 4.5 (e.u)^2 - 1.5 u.u; for
+// e_x = 0, A +- B is one fused multiply-add on A.
 template <int K, typename V>
 __device__ __forceinline__ void lp_pair(V (&r)[Q], const LpParams &k, V dr, V Srho, V nusq15, const V (&a0)[2],
                                         const V (&beu)[2], V u0, V u1, V u2)
@@ -167,17 +168,19 @@ __device__ __forceinline__ void lp_pair(V (&r)[Q], const LpParams &k, V dr, V Sr
     const V eu = lp_eu<a>(u0, u1, u2);
     const V t = vfma(vmul(vsplat<V>(4.5f), eu), eu, nusq15);
     const V X = vfma(Srho, t, dr);
-    V A, B;
-    if (ex == 0) {
-        A = vfma(vsplat<V>(k.wom[cls]), X, a0[cls]);
-        B = vmul(beu[cls], eu);
-    } else {
-        A = vfma(vsplat<V>(k.wom[cls]), X, vfma(vsplat<V>(ex > 0 ? k.a_eu[cls] : -k.a_eu[cls]), eu, a0[cls]));
-        B = vfma(beu[cls], eu, vsplat<V>(ex > 0 ? k.b_ex[cls] : -k.b_ex[cls]));
-    }
     const V om1 = vsplat<V>(k.om1);
-    r[a] = vfma(om1, r[a], vadd(A, B));
-    r[b] = vfma(om1, r[b], vsub(A, B));
+    if (ex == 0) {
+        // A +- B with B = beu e.u as one fused operation each (a separate
+        // product and sum is what the compiler may fuse on the packed pipe)
+        const V A = vfma(vsplat<V>(k.wom[cls]), X, a0[cls]);
+        r[a] = vfma(om1, r[a], vfma(beu[cls], eu, A));
+        r[b] = vfma(om1, r[b], vfma(vneg(beu[cls]), eu, A));
+    } else {
+        const V A = vfma(vsplat<V>(k.wom[cls]), X, vfma(vsplat<V>(ex > 0 ? k.a_eu[cls] : -k.a_eu[cls]), eu, a0[cls]));
+        const V B = vfma(beu[cls], eu, vsplat<V>(ex > 0 ? k.b_ex[cls] : -k.b_ex[cls]));
+        r[a] = vfma(om1, r[a], vadd(A, B));
+        r[b] = vfma(om1, r[b], vsub(A, B));
+    }
 }
 
 // In place on raw values r[19] of one storage type with scale S.  emit(a)

@@ -208,9 +208,12 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *smem)
 // mode 0: after a step (logs, advances the step counter);
 // mode 1: initial reduction of a freshly loaded state (force and shift of
 //         the current step from the reader-side totals, nothing logged).
+// step < 0 (mode 0): the step is read from the step counter (the tail is
+// its only writer, once per step).
 static __device__ __forceinline__ void step_tail(const StepArgs &a, long long step, double force_used, int mode, double *smem,
                                                  int nthreads)
 {
+    if (step < 0) step = __ldcg(a.step_ctr);
     const int nz = a.nz;
     const double np = (double)a.nx * (double)a.ny;
     const double *cshift = a.shift + (size_t)(step & 1) * nz * 3;

@@ -52,12 +52,12 @@ struct PersistArgs {
     unsigned *arrivals;            // grid-barrier arrivals (zero at launch)
     int *abort;                    // a bounded wait gave up: the launch stops
     unsigned long long wait_ns;    // limit of every bounded wait
-    int withhold;                  // test switch (0 otherwise): block 0 withholds its first load
+    int withhold;                  // test switch (0 otherwise): the first item's first load is withheld
 };
 
 // Per-stage header, written by the producer before it arms the stage: the
-// channel's arguments and everything the consumers need for the stage's
-// work, so they read no global memory to find it.
+// channel's arguments and the item and row group of the stage, so the
+// consumers find their work without a global-memory round trip.
 struct StageHeader {
     ChannelLaunch L;  // the item's channel (copied when the stage held another)
     BatchItem it;
@@ -66,9 +66,6 @@ struct StageHeader {
     int z, y0;        // plane and first row of the group (kind 1: plane, unused)
     int chan;         // channel whose arguments L holds
     int pad_;
-    long long step;   // the channel's step counter
-    double G;         // the force of this step
-    double sh[3];     // the plane's shift (previous plane means)
 };
 
 // Shared memory after the stages: full[S], empty[S] (8 bytes each), then
@@ -109,9 +106,10 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
 {
     const int S = a.stages;
     int i = 0;            // stage sequence number within the step
-    // test switch: block 0 neither arms nor loads its first row group of the
-    // first step, so its consumers' wait runs out with no copy in flight
-    bool withhold = a.withhold != 0 && blockIdx.x == 0 && s == 0;
+    // test switch: the block that takes the first item of the first step
+    // neither arms nor loads its first row group, so its consumers' wait runs
+    // out with no copy in flight
+    const bool withhold_step = a.withhold != 0 && s == 0;
     unsigned loaded = 0;  // bit st: a load into stage st was issued (its phase is the last one armed)
     unsigned phase = 0;   // bit st: parity of that phase
     // once the consumers have released sequence seq, store the row group it held
@@ -148,19 +146,12 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
             for (int w = lane; w < (int)(sizeof(ChannelLaunch) / sizeof(int)); w += 32) dst[w] = __ldg(src + w);
         }
         if (lane == 0) {
-            const StepArgs &p = a.chans[it.chan].p;
             H.it = it;
             H.item = h;
             H.group = g;
             H.z = z;
             H.y0 = y0;
             H.chan = it.chan;
-            H.step = __ldcg(p.step_ctr);
-            H.G = p.const_q ? __ldcg(p.force + (H.step & 1)) : p.gx;
-            const double *shp = p.shift + (size_t)(H.step & 1) * p.nz * 3 + z * 3;
-            H.sh[0] = __ldcg(shp);
-            H.sh[1] = __ldcg(shp + 1);
-            H.sh[2] = __ldcg(shp + 2);
         }
         __syncwarp();
     };
@@ -189,8 +180,7 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
                     gr = L.textured ? group_rows<ODD, 1>(L.p, lane, y0, z, wall)
                                     : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
                 const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && gr.bulk);
-                const bool issue = __shfl_sync(0xffffffffu, *s_abort, 0) == 0 && !withhold;
-                withhold = false;
+                const bool issue = __shfl_sync(0xffffffffu, *s_abort, 0) == 0 && !(withhold_step && h == 0 && g == 0);
                 if (issue) {
                     fill(st, h, it, g, z, y0);
                     if (lane == 0) mbar_expect_tx(full + st, (uint32_t)((size_t)__popc(vote) * k * L.t.row_bytes));
@@ -246,15 +236,21 @@ __device__ __forceinline__ void persist_links(const StepArgs &p, const BatchItem
 }
 
 template <typename T, bool ODD, bool ANYQ>
-__device__ __forceinline__ void persist_consumers(const PersistArgs &a, unsigned char *smem, uint64_t *full,
+__device__ __forceinline__ void persist_consumers(const PersistArgs &a, int s, unsigned char *smem, uint64_t *full,
                                                   uint64_t *empty, const StageHeader *hdr, int nc,
                                                   volatile int *s_abort)
 {
     using LpT = typename std::conditional<std::is_same<T, double>::value, float, T>::type;
     const int S = a.stages;
+    // parity of the step counter (every channel of a batch is at the same
+    // step, and a loaded state starts at step 0 with the even AA step)
+    const int sp = (a.first_odd + s) & 1;
     double acc[NP];
 #pragma unroll
     for (int q = 0; q < NP; ++q) acc[q] = 0.0;
+    // per item: the force of the step and the plane's shift (the previous
+    // plane means), read once at the item's first stage
+    double G = 0.0, sh[3] = {0.0, 0.0, 0.0};
     for (int i = 0;; ++i) {
         const int st = i % S;
         int bad = 0;
@@ -267,28 +263,35 @@ __device__ __forceinline__ void persist_consumers(const PersistArgs &a, unsigned
         if (H.item < 0) return;  // end of the step (the same header for every consumer)
         const StepArgs &p = H.L.p;
         const bool q = ANYQ && p.const_q != 0;  // a batch without constant-Q channels compiles no such path
-        const double G = H.G;
         const int z = H.z;
+        if (H.group <= 0) {  // an item's first stage
+            G = q ? __ldcg(p.force + sp) : p.gx;
+            const double *shp = p.shift + (size_t)sp * p.nz * 3 + z * 3;
+            sh[0] = __ldcg(shp);
+            sh[1] = __ldcg(shp + 1);
+            sh[2] = __ldcg(shp + 2);
+        }
         if (H.group < 0) {
-            if (q) persist_links<T, ODD, true>(p, H.it, G, H.sh, acc, nc);
-            else persist_links<T, ODD, false>(p, H.it, G, H.sh, acc, nc);
+            if (q) persist_links<T, ODD, true>(p, H.it, G, sh, acc, nc);
+            else persist_links<T, ODD, false>(p, H.it, G, sh, acc, nc);
         } else {
             const int k = min(H.L.t.k, p.ny - H.y0);
             const int dstride = H.L.t.dir_elems;
             T *sb = reinterpret_cast<T *>(smem + (size_t)st * a.stage_bytes);
             [[maybe_unused]] const LpParams lk = lp_params<LpT>((float)p.omega, (float)G);
             if (q) {
-                if (H.L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
-                else consume_group<T, ODD, true, false>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
+                if (H.L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
+                else consume_group<T, ODD, true, false>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
             } else {
-                if (H.L.textured) consume_group<T, ODD, false, true>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
-                else consume_group<T, ODD, false, false>(p, lk, sb, dstride, H.y0, k, z, G, H.sh, acc, nc);
+                if (H.L.textured) consume_group<T, ODD, false, true>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
+                else consume_group<T, ODD, false, false>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
             }
             fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         }
         const bool done = H.group < 0 || H.group == H.it.count - 1;
         if (done) {  // the item is done: its plane contribution (the stage is released after it)
-            plane_contribute(p, acc, z, H.it.slot, H.it.ncontrib, H.step, G, 0, nc);
+            // step -1: the channel's step tail reads its own step counter
+            plane_contribute(p, acc, z, H.it.slot, H.it.ncontrib, -1, G, 0, nc);
 #pragma unroll
             for (int r = 0; r < NP; ++r) acc[r] = 0.0;
         }
@@ -314,7 +317,7 @@ __device__ __forceinline__ void persist_step(const PersistArgs &a, int s, unsign
     }
     __syncthreads();
     if (threadIdx.x >= nc) persist_producer<T, ODD>(a, s, threadIdx.x - nc, smem, full, empty, hdr, s_abort);
-    else persist_consumers<T, ODD, ANYQ>(a, smem, full, empty, hdr, nc, s_abort);
+    else persist_consumers<T, ODD, ANYQ>(a, s, smem, full, empty, hdr, nc, s_abort);
 }
 
 // Grid-wide barrier between steps (all blocks are resident: cooperative

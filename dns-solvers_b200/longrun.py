@@ -26,6 +26,14 @@ Averaged over the window (after --spinup steps), per run:
     over slip and over no-slip wall cells at the end of the window.
 Errors against FP64: max |profile - profile_64| / max |profile_64| and the
 relative differences of Re_tau, C_f, U_b.
+
+The window is cut into --blocks equal blocks whose averages are kept: the
+spread of the block averages gives each quantity's standard error (batch
+means), so a difference is stated with the sampling error it must beat --
+"sigma" (the combined standard error of the two runs' averages) and
+"z" = |difference| / sigma.  The profiles are also folded about the channel
+centre (the two half-channels are statistically the same), which halves
+their sampling variance; "*_fold_*" entries use the folded profiles.
 """
 from __future__ import annotations
 
@@ -44,7 +52,7 @@ import dnslbm  # noqa: E402
 import inputs  # noqa: E402
 
 
-def run_one(wl, s0, flags, prec, spinup, steps, sample, device=0):
+def run_one(wl, s0, flags, prec, spinup, steps, sample, blocks=1, device=0):
     bc = dnslbm.BC_GENERAL if inputs.needs_general(wl) else dnslbm.BC_REFERENCE
     ch = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, gx=wl.gx, force_mode=dnslbm.CONST_G, precision=prec,
                         bc_mode=bc, device=device)
@@ -57,33 +65,46 @@ def run_one(wl, s0, flags, prec, spinup, steps, sample, device=0):
         n = min(4000, left)
         ch.step(n)
         left -= n
-    stress, flow, rho = [], [], []
-    ch.stats_reset()
-    done = 0
-    while done < steps:
-        n = min(sample, steps - done)
-        first = ch.steps_done
-        ch.step(n)
-        lg = ch.logs(first, n)
-        stress.append(lg[:, dnslbm.LOG_NAMES.index("stress")])
-        flow.append(lg[:, dnslbm.LOG_NAMES.index("flowrate")])
-        rho.append(lg[:, dnslbm.LOG_NAMES.index("rho")])
-        done += n
-        ch.stats_accumulate()
-    secs = time.perf_counter() - t0
-    vel, _ = ch.moments()
-    st, _ = ch.stats_average()
-    ch.close()
-    stress, flow, rho = np.concatenate(stress), np.concatenate(flow), np.concatenate(rho)
     nu = (2.0 / wl.omega - 1.0) / 6.0
     h = wl.nz / 2.0
-    tau_w = float(np.mean(stress))
-    rho_m = float(np.mean(rho))
-    utau = math.sqrt(abs(tau_w) / rho_m)
-    ub = float(np.mean(flow)) / (wl.ny * wl.nz)
-    out = {"precision": prec, "seconds": round(secs, 2), "tau_w": tau_w, "u_tau": utau, "re_tau": utau * h / nu,
-           "u_bulk": ub, "cf": 2 * tau_w / (rho_m * ub * ub), "mean_u": st[0, 1:-1], "u_rms": st[3, 1:-1],
-           "v_rms": st[4, 1:-1], "w_rms": st[5, 1:-1]}
+    per_block = steps // blocks
+    bq = []  # per block: the scalars and profiles averaged over the block
+    for _b in range(blocks):
+        stress, flow, rho = [], [], []
+        ch.stats_reset()
+        done = 0
+        while done < per_block:
+            n = min(sample, per_block - done)
+            first = ch.steps_done
+            ch.step(n)
+            lg = ch.logs(first, n)
+            stress.append(lg[:, dnslbm.LOG_NAMES.index("stress")])
+            flow.append(lg[:, dnslbm.LOG_NAMES.index("flowrate")])
+            rho.append(lg[:, dnslbm.LOG_NAMES.index("rho")])
+            done += n
+            ch.stats_accumulate()
+        st, _ = ch.stats_average()
+        stress, flow, rho = np.concatenate(stress), np.concatenate(flow), np.concatenate(rho)
+        tau_w = float(np.mean(stress))
+        rho_m = float(np.mean(rho))
+        utau = math.sqrt(abs(tau_w) / rho_m)
+        ub = float(np.mean(flow)) / (wl.ny * wl.nz)
+        bq.append({"tau_w": tau_w, "u_tau": utau, "re_tau": utau * h / nu, "u_bulk": ub,
+                   "cf": 2 * tau_w / (rho_m * ub * ub), "mean_u": st[0, 1:-1], "u_rms": st[3, 1:-1],
+                   "v_rms": st[4, 1:-1], "w_rms": st[5, 1:-1]})
+    secs = time.perf_counter() - t0
+    vel, _ = ch.moments()
+    ch.close()
+    out = {"precision": prec, "seconds": round(secs, 2), "blocks": blocks}
+    for k in bq[0]:
+        vals = np.array([b[k] for b in bq])
+        out[k] = vals.mean(axis=0) if vals.ndim > 1 else float(vals.mean())
+        se = vals.std(axis=0, ddof=1) / math.sqrt(blocks) if blocks > 1 else np.zeros_like(vals[0])
+        out[k + "_se"] = se if vals.ndim > 1 else float(se)
+        if vals.ndim > 1:  # folded about the centre plane
+            fv = 0.5 * (vals + vals[:, ::-1])
+            out[k + "_fold"] = fv.mean(axis=0)
+            out[k + "_fold_se"] = fv.std(axis=0, ddof=1) / math.sqrt(blocks) if blocks > 1 else np.zeros_like(fv[0])
     slip = flags[:, :, 0] == -2
     if slip.any():
         u1 = vel[:, :, 1, 0]
@@ -94,10 +115,22 @@ def run_one(wl, s0, flags, prec, spinup, steps, sample, device=0):
 
 def compare(ref, o):
     def prof(k):
-        return float(np.max(np.abs(o[k] - ref[k])) / max(np.max(np.abs(ref[k])), 1e-300))
-    e = {f"{k}_max_rel": prof(k) for k in ("mean_u", "u_rms", "v_rms", "w_rms")}
+        scale = max(np.max(np.abs(ref[k])), 1e-300)
+        d = np.abs(o[k] - ref[k])
+        sig = np.sqrt(ref[k + "_se"] ** 2 + o[k + "_se"] ** 2)
+        i = int(np.argmax(d))
+        return float(d[i] / scale), float(np.max(sig) / scale), float(np.max(d / np.maximum(sig, 1e-300)))
+    e = {}
+    for k in ("mean_u", "u_rms", "v_rms", "w_rms"):
+        for name in (k, k + "_fold"):
+            rel, sig, z = prof(name)
+            e[f"{name}_max_rel"] = rel
+            e[f"{name}_sigma_rel"] = sig
+            e[f"{name}_max_z"] = z
     for k in ("re_tau", "cf", "u_bulk", "tau_w"):
         e[f"{k}_rel"] = abs(o[k] - ref[k]) / abs(ref[k])
+        sig = math.sqrt(ref[k + "_se"] ** 2 + o[k + "_se"] ** 2)
+        e[f"{k}_sigma_rel"] = sig / abs(ref[k])
     if "slip_u_first_plane" in ref:
         e["slip_u_rel"] = abs(o["slip_u_first_plane"] - ref["slip_u_first_plane"]) / abs(ref["slip_u_first_plane"])
     return e
@@ -109,6 +142,7 @@ def main():
     ap.add_argument("--spinup", type=int, default=0, help="steps before the averaging window")
     ap.add_argument("--steps", type=int, default=50000, help="steps in the averaging window")
     ap.add_argument("--sample", type=int, default=100)
+    ap.add_argument("--blocks", type=int, default=10, help="window blocks for the standard errors")
     ap.add_argument("--precisions", default="64,64p,32,16",
                     help="64p: FP64 control from a perturbed field (64pA: perturbation amplitude A)")
     ap.add_argument("--control-amp", type=float, default=1e-7, help="relative perturbation of the 64p control")
@@ -130,15 +164,15 @@ def main():
             if inputs.needs_general(wl):
                 init = inputs.rest_solids(init, flags)
         try:
-            r = run_one(wl, init, flags, int(p[:2]), a.spinup, a.steps, a.sample)
+            r = run_one(wl, init, flags, int(p[:2]), a.spinup, a.steps, a.sample, a.blocks)
         except dnslbm.DnsLbmError as e:  # e.g. a NaN wall stress: reported, not fatal
             r = {"failed": str(e)}
         r["run"] = p
         runs.append(r)
     ref = runs[0]
     summary = {"workload": wl.name, "grid": f"{wl.nx}x{wl.nz + 2}x{wl.ny}", "texture": wl.texture,
-               "spinup": a.spinup, "steps": a.steps, "sample_every": a.sample, "seed": a.seed,
-               "control_amp": a.control_amp, "runs": []}
+               "command": " ".join(sys.argv), "spinup": a.spinup, "steps": a.steps, "sample_every": a.sample,
+               "blocks": a.blocks, "seed": a.seed, "control_amp": a.control_amp, "runs": []}
     if inputs.needs_general(wl):
         summary["note"] = ("walls with riblets: the reference's wall-stress formula (a one-sided difference of "
                            "plane means at a flat wall) does not measure the riblet drag; compare u_bulk at "

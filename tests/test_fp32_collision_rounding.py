@@ -66,12 +66,13 @@ def collide_f32(r, omega, g, unbiased):
         ex = E[a, 0]
         if ex == 0:
             A = fma(w * om, X, f32(-3) * w * G * u[0])
-            B = beu * eu
+            out[a] = fma(om1, r[a], fma(beu, eu, A))
+            out[b] = fma(om1, r[b], fma(-beu, eu, A))
         else:
             A = fma(w * om, X, fma(f32(9) * w * G * ex, eu, f32(-3) * w * G * u[0]))
             B = fma(beu, eu, f32(3) * w * G * ex)
-        out[a] = fma(om1, r[a], A + B)
-        out[b] = fma(om1, r[b], A - B)
+            out[a] = fma(om1, r[a], A + B)
+            out[b] = fma(om1, r[b], A - B)
     return out
 
 
