@@ -25,6 +25,7 @@ void launch_stats(int precision, const IoArgs &p, dim3 grid, dim3 block, int row
 void launch_stats_sample(int nz, double np, const double *planes, double *mean, double *acc, bool accumulate,
                          cudaStream_t s);
 void launch_stats_rows(int nz, double np, const double *mean, const double *planes, double *out, cudaStream_t s);
+void launch_quadrant(const double *vel, int nx, int ny, int zd, double *mean, double *out, cudaStream_t s);
 int persist_prepare_f64(size_t smem);
 int persist_occupancy_f64(int threads, size_t smem, bool any_q);
 cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, bool any_q, cudaStream_t s);
@@ -107,6 +108,7 @@ struct dnslbm_ctx {
     cudaStream_t out_stream = nullptr;
     cudaEvent_t out_ev[2] = {nullptr, nullptr};
     int out_pending = 0;
+    double *quad_buf = nullptr;  // quadrant analysis: plane means [zd][3], plane sums [zd][9]
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> tev;  // per-launch timing events
     dim3 grid, block;
@@ -202,7 +204,7 @@ static void free_all(dnslbm_ctx *c)
                     c->plane_sums, c->logs,       c->step_ctr,      c->status,      c->plane_ctr,
                     c->total_ctr,  c->staging,    c->stat_partials, c->stat_planes, c->stat_mean,
                     c->band_of,    c->links,      c->plane_list,    c->d_llaunch,   c->stat_acc,
-                    c->out_lbf,    c->out_vel,    c->out_den,       c->out_stats};
+                    c->out_lbf,    c->out_vel,    c->out_den,       c->out_stats,   c->quad_buf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : c->ev)
@@ -249,6 +251,7 @@ static void tma_layout(dnslbm_ctx *c)
 
 // seg > 0 (FP64 only): groups are x-segments of seg elements (even) of one
 // row, for rows too long for two whole-row stages.
+constexpr int kMaxSegments = 4;
 static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bps, int seg = 0)
 {
     const int row_bytes = c->pitch * (int)c->esize;
@@ -257,6 +260,7 @@ static int tma_configure(dnslbm_ctx *c, int k, int stages, int consumers, int bp
     if (seg > 0 && (c->deck.precision != 64 || seg % 2 || seg >= c->nx)) return -1;
     if (seg > 0) k = 1;
     const int nseg = seg > 0 ? (c->nx + seg - 1) / seg : 1;
+    if (nseg > kMaxSegments) return -1;  // more groups per plane than partial-sum slots
     const int dir_elems = seg > 0 ? seg + 4 : k * c->pitch;  // a segment keeps a halo of 2 elements a side
     const size_t smem_stage = (size_t)Q * dir_elems * c->esize;
     int maxsmem = 0, nsm = 0;
@@ -385,7 +389,10 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     if (bx > 128) bx = 128;
     c->block = dim3(bx, 1, 1);
     c->grid = dim3((c->nx + bx - 1) / bx, (c->ny + c->rows - 1) / c->rows, c->nz);
-    c->slots = (int)(c->grid.x * c->grid.y);
+    // partial-sum slots per plane: enough for the per-thread kernels and for
+    // any split of a plane's row groups among blocks (at most one per group,
+    // plus one; x-segmented FP64 rows: kMaxSegments groups per row)
+    c->slots = std::max((int)(c->grid.x * c->grid.y), (deck->precision == 64 ? kMaxSegments : 1) * c->ny + 1);
     {
         // Row-pipelined step.  A stage holds a group of k consecutive rows of
         // one plane for all 19 directions.  Defaults measured on a B200
@@ -412,16 +419,13 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
             if (const char *e = getenv("DNSLBM_SEGMENT")) seg = atoi(e) & ~1;
             if (seg > 0 || tma_configure(c, k, stages, consumers, bps)) {
                 // FP64 rows too long for two whole-row stages: x-segments
-                for (int nseg = 2; seg == 0 && c->deck.precision == 64 && nseg <= 8; ++nseg)
+                for (int nseg = 2; seg == 0 && c->deck.precision == 64 && nseg <= kMaxSegments; ++nseg)
                     if (!tma_configure(c, 1, stages, consumers, bps, segment_for(c->nx, nseg))) break;
                 if (seg > 0) tma_configure(c, 1, stages, consumers, bps, seg);
             }
         }
         describe_kernel(c);
     }
-    // partial-sum slots: enough for the per-thread kernels and for any row
-    // group split the tuner may choose
-    c->slots = std::max(c->slots, c->ny + 1);
     const size_t nblocks = (size_t)c->nz * c->slots;
 
     struct Alloc { void **p; size_t bytes; };
@@ -1142,6 +1146,79 @@ extern "C" int dnslbm_output_begin(dnslbm_ctx *c, double *state, double *vel, do
                            c->out_stream));
     CK(cudaEventRecord(c->out_ev[1], c->out_stream));
     c->out_pending = 1;
+    return DNSLBM_OK;
+}
+
+// ---------------------------------------------------------------- post-processing
+// Quadrant analysis (quadrant-analysis/src/qUADrantA.c:140-170): from the
+// per-plane sums of quadrant_kernel to the reference's output arrays.
+static void quadrant_finish(int zd, double n, const double *sums, double *quadrant, double *dquadrant, double *uw)
+{
+    for (int i = 0; i < 4 * zd; ++i) {
+        if (quadrant) quadrant[i] = 0.0;
+        if (dquadrant) dquadrant[i] = 0.0;
+    }
+    for (int k = 0; k < zd; ++k)
+        if (uw) uw[k] = 0.0;
+    for (int k = 1; k < zd - 1; ++k) {
+        const double *p = sums + (size_t)k * 9;
+        for (int a = 0; a < 4; ++a) {
+            if (quadrant) quadrant[a * zd + k] = p[a] / p[4 + a];  // an empty quadrant gives 0/0, as the reference
+            if (dquadrant) dquadrant[a * zd + k] = p[a] / n;
+        }
+        if (uw) uw[k] = p[8] / n;
+    }
+}
+
+extern "C" int dnslbm_quadrant(dnslbm_ctx *c, double *quadrant, double *dquadrant, double *uw)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    CK(cudaSetDevice(c->deck.device));
+    const int zd = c->nz + 2;
+    const size_t cells = (size_t)c->nx * c->ny * zd;
+    int rc;
+    if ((rc = out_alloc(c, &c->out_vel, cells * 3)) || (rc = out_alloc(c, &c->out_den, cells)) ||
+        (rc = out_alloc(c, &c->quad_buf, (size_t)zd * 12)))
+        return rc;
+    CK(cudaDeviceSynchronize());
+    // the velocity field in the vel layout, then the two plane passes
+    if (c->out_pending) CK(cudaStreamWaitEvent(c->stream, c->out_ev[1], 0));
+    launch_io(c->deck.precision, 3, io_args(c), 0, c->nx, c->out_vel, c->out_den, c->stream);
+    launch_quadrant(c->out_vel, c->nx, c->ny, zd, c->quad_buf, c->quad_buf + (size_t)zd * 3, c->stream);
+    CK(cudaGetLastError());
+    std::vector<double> sums((size_t)zd * 9);
+    CK(cudaMemcpyAsync(sums.data(), c->quad_buf + (size_t)zd * 3, sums.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    quadrant_finish(zd, (double)c->nx * c->ny, sums.data(), quadrant, dquadrant, uw);
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_quadrant_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *quadrant,
+                                   double *dquadrant, double *uw)
+{
+    dnslbm_ctx *c = nullptr;  // errors go to dnslbm_last_error(NULL)
+    if (!vel) return fail(c, DNSLBM_ERR_ARG, "null velocity field");
+    if (xdv < 1 || ydv < 1 || zdv < 1) return fail(c, DNSLBM_ERR_ARG, "grid %dx%dx%d too small", xdv, ydv, zdv);
+    const int zd = zdv + 2;
+    const size_t n = (size_t)xdv * ydv * zd * 3;
+    CK(cudaSetDevice(device));
+    double *dv = nullptr, *buf = nullptr;
+    cudaError_t e = cudaMalloc(&dv, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&buf, (size_t)zd * 12 * sizeof(double));
+    std::vector<double> sums((size_t)zd * 9);
+    if (e == cudaSuccess) e = cudaMemcpy(dv, vel, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        launch_quadrant(dv, xdv, ydv, zd, buf, buf + (size_t)zd * 3, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(sums.data(), buf + (size_t)zd * 3, sums.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    if (dv) cudaFree(dv);
+    if (buf) cudaFree(buf);
+    if (e != cudaSuccess) return fail(c, DNSLBM_ERR_CUDA, "quadrant analysis of a velocity field: %s", cudaGetErrorString(e));
+    quadrant_finish(zd, (double)xdv * ydv, sums.data(), quadrant, dquadrant, uw);
     return DNSLBM_OK;
 }
 

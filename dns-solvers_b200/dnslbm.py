@@ -78,6 +78,8 @@ def lib():
     L.dnslbm_moments.argtypes = [vp, dp, dp]
     L.dnslbm_step_timed.argtypes = [vp, ctypes.c_long, dp, dp, dp]
     L.dnslbm_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    L.dnslbm_quadrant.argtypes = [vp, dp, dp, dp]
+    L.dnslbm_quadrant_vel.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.dnslbm_output_begin.argtypes = [vp, dp, dp, dp, dp]
     L.dnslbm_output_wait.argtypes = [vp]
     L.dnslbm_set_wait_limit.argtypes = [vp, ctypes.c_double]
@@ -195,6 +197,14 @@ class Channel:
         t, e, o = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         self._ck(self.L.dnslbm_step_timed(self.h, n, ctypes.byref(t), ctypes.byref(e), ctypes.byref(o)))
         return t.value, e.value, o.value
+
+    def quadrant(self):
+        """Quadrant analysis of the current state: (quadrant[4][zd],
+        dquadrant[4][zd], uw[zd]) as the reference's quadrant files."""
+        zd = self.shape[2] + 2
+        q, dq, uw = np.zeros((4, zd)), np.zeros((4, zd)), np.zeros(zd)
+        self._ck(self.L.dnslbm_quadrant(self.h, _dp(q), _dp(dq), _dp(uw)))
+        return q, dq, uw
 
     def output_begin(self, state=None, vel=None, den=None, stats=None):
         """Start the asynchronous output of the current state into the given
@@ -398,3 +408,16 @@ class PinnedArray:
             self.ptr = None
 
     __del__ = free
+
+
+def quadrant_vel(vel, device=0):
+    """Quadrant analysis of a velocity field [xdv][ydv][zd][3] on the GPU."""
+    L = lib()
+    v = np.ascontiguousarray(vel, np.float64)
+    nx, ny, zd, three = v.shape
+    assert three == 3
+    q, dq, uw = np.zeros((4, zd)), np.zeros((4, zd)), np.zeros(zd)
+    rc = L.dnslbm_quadrant_vel(_dp(v), nx, ny, zd - 2, device, _dp(q), _dp(dq), _dp(uw))
+    if rc:
+        raise DnsLbmError(rc, L.dnslbm_last_error(None).decode())
+    return q, dq, uw

@@ -19,6 +19,10 @@
  *   RIBH RIBS (riblet height and spacing; riblets select the general wall
  *   rule, DNSLBM_BC_GENERAL)
  *   PRECISION 64|32|16   FORCE q|g   GX   DEVICE   OMEGA (overrides Rebs)
+ *   QUADRANT 1  also the quadrant analysis of quadrant-analysis/src/
+ *               qUADrantA.c at every output event, on the GPU, from the live
+ *               state: quadrant.000.TTTT and dquadrant.000.TTTT ([4][zd] then
+ *               [zd] doubles)
  *   ASYNC 1|0   output without stopping the time loop (default 1): at an
  *               output step the library computes the outputs on the GPU and
  *               copies them to page-locked host buffers while the next steps
@@ -48,7 +52,7 @@
 typedef struct {
     double Rebs, ub, CFL, GX, OMEGA;
     int zdv, ydv, xdv, TSTR, TEND, ITER, RSLIP, PSLIP;
-    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS, ASYNC;
+    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS, ASYNC, QUADRANT;
     char TEXTURE[32], FORCE[8];
 } Deck;
 
@@ -86,7 +90,7 @@ static int deck_set(Deck *d, const char *k, const char *v)
 #define STR(N) if (!strcmp(k, #N)) { snprintf(d->N, sizeof d->N, "%s", v); return 0; }
     DBL(Rebs) DBL(ub) DBL(CFL) DBL(GX) DBL(OMEGA)
     INT(zdv) INT(ydv) INT(xdv) INT(TSTR) INT(TEND) INT(ITER) INT(RSLIP) INT(PSLIP)
-    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS) INT(ASYNC)
+    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS) INT(ASYNC) INT(QUADRANT)
     STR(TEXTURE) STR(FORCE)
 #undef DBL
 #undef INT
@@ -377,6 +381,24 @@ int main(int argc, char **argv)
             sn->label = TM + ss / utime;
             sn->checkpoint = !(ss % (10 * utime));
             if (sn->checkpoint && (rc = dnslbm_get_force(c, &sn->force))) return die(c, rc, "dnslbm_get_force");
+            if (D.QUADRANT) {
+                double *q = malloc(9 * (size_t)zd * sizeof(double));
+                if (!q) return die(c, DNSLBM_ERR_IO, "host allocation");
+                if ((rc = dnslbm_quadrant(c, q, q + 4 * zd, q + 8 * zd))) return die(c, rc, "dnslbm_quadrant");
+                char qn[64];
+                snprintf(qn, sizeof qn, "quadrant.%.3d.%.4d", 0, (int)sn->label);
+                FILE *qf = fopen(qn, "wb");
+                int bad = !qf || fwrite(q, sizeof(double), 4 * (size_t)zd, qf) != 4 * (size_t)zd ||
+                          fwrite(q + 8 * zd, sizeof(double), zd, qf) != (size_t)zd;
+                if (qf) bad |= fclose(qf) != 0;
+                snprintf(qn, sizeof qn, "dquadrant.%.3d.%.4d", 0, (int)sn->label);
+                qf = fopen(qn, "wb");
+                bad |= !qf || fwrite(q + 4 * zd, sizeof(double), 4 * (size_t)zd, qf) != 4 * (size_t)zd ||
+                       fwrite(q + 8 * zd, sizeof(double), zd, qf) != (size_t)zd;
+                if (qf) bad |= fclose(qf) != 0;
+                free(q);
+                if (bad) return die(c, DNSLBM_ERR_IO, qn);
+            }
             if (D.ASYNC) {
                 /* the previous event's copies have landed (the steps since
                  * took longer); hand them to the writer once it is done with

@@ -180,6 +180,23 @@ int dnslbm_output_begin(dnslbm_ctx *ctx, double *state, double *vel, double *den
 /* Block until the copies of the last dnslbm_output_begin have landed. */
 int dnslbm_output_wait(dnslbm_ctx *ctx);
 
+/* Quadrant analysis of the current state, on the GPU
+ * (quadrant-analysis/src/qUADrantA.c): per wall-normal plane, the
+ * fluctuations u' = u - <u>, w' = w - <w> of the cell velocities (those
+ * dnslbm_moments returns) split into the quadrants Q1 (u'>0, w'>0),
+ * Q2 (u'<0, w'>0), Q3 (u'<0, w'<0), Q4 (u'>0, w'<0):
+ *   quadrant[4][zd]   the conditional mean of u'w' in each quadrant,
+ *   dquadrant[4][zd]  each quadrant's contribution (its sum / cells of the plane),
+ *   uw[zd]            the plane mean of u'w',
+ * wall planes 0 -- the reference's quadrant.000.TTTT file holds quadrant
+ * then uw, dquadrant.000.TTTT dquadrant then uw.  Any pointer may be NULL. */
+int dnslbm_quadrant(dnslbm_ctx *ctx, double *quadrant, double *dquadrant, double *uw);
+/* The same for a velocity field read from a vel.NNNN file
+ * ([xdv][ydv][zdv+2][3] doubles), on CUDA device `device` (temporary device
+ * memory, freed before return; errors in dnslbm_last_error(NULL)). */
+int dnslbm_quadrant_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *quadrant, double *dquadrant,
+                        double *uw);
+
 /* Timing support for benchmarks: advance nsteps like dnslbm_step and return
  * CUDA-event times on the context's stream: total, and the summed device
  * time of the two step kernels (even / odd parity launches). */

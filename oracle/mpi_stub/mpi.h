@@ -42,10 +42,11 @@ typedef FILE *MPI_File;
 #define MPI_MODE_CREATE 4
 #define MPI_SUCCESS 0
 
-/* predefined datatypes are handles 1..3; derived types are appended */
+/* predefined datatypes are handles 1..4; derived types are appended */
 #define MPI_CHAR 1
 #define MPI_INT 2
 #define MPI_DOUBLE 3
+#define MPI_INTEGER 4  /* the Fortran INTEGER handle, 4 bytes here */
 
 int MPI_Init(int *argc, char ***argv);
 int MPI_Finalize(void);
@@ -55,6 +56,7 @@ int MPI_Comm_rank(MPI_Comm c, int *rank);
 int MPI_Barrier(MPI_Comm c);
 int MPI_Bcast(void *buf, int count, MPI_Datatype t, int root, MPI_Comm c);
 int MPI_Allreduce(const void *s, void *r, int count, MPI_Datatype t, MPI_Op op, MPI_Comm c);
+int MPI_Reduce(const void *s, void *r, int count, MPI_Datatype t, MPI_Op op, int root, MPI_Comm c);
 int MPI_Cart_create(MPI_Comm old, int nd, const int *dims, const int *periods, int reorder, MPI_Comm *cart);
 int MPI_Cart_coords(MPI_Comm c, int rank, int maxdims, int *coords);
 int MPI_Cart_rank(MPI_Comm c, const int *coords, int *rank);

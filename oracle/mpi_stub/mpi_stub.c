@@ -10,8 +10,8 @@
 
 /* ---- datatypes: a handle indexes a table of byte sizes ------------------ */
 #define MAX_TYPES 4096
-static long long type_bytes[MAX_TYPES] = {0, 1, 4, 8};
-static int n_types = 4;
+static long long type_bytes[MAX_TYPES] = {0, 1, 4, 8, 4};
+static int n_types = 5;
 
 static long long tsize(MPI_Datatype t)
 {
@@ -67,6 +67,14 @@ int MPI_Bcast(void *buf, int count, MPI_Datatype t, int root, MPI_Comm c)
 int MPI_Allreduce(const void *s, void *r, int count, MPI_Datatype t, MPI_Op op, MPI_Comm c)
 {
     (void)op; (void)c;
+    memmove(r, s, (size_t)(count * tsize(t)));
+    return MPI_SUCCESS;
+}
+
+/* one rank: the reduction of one contribution is that contribution */
+int MPI_Reduce(const void *s, void *r, int count, MPI_Datatype t, MPI_Op op, int root, MPI_Comm c)
+{
+    (void)op; (void)root; (void)c;
     memmove(r, s, (size_t)(count * tsize(t)));
     return MPI_SUCCESS;
 }

@@ -24,6 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblbmoracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "dnsref")
+QUAD_BIN = os.path.join(HERE, "_ref", "quadref")
 # the reference's DNS-solver/src directory (the one place it is named; the
 # Makefile's REF_SRC gets the same value)
 REF_SRC = os.environ.get("REF_SRC", "/root/reference/DNS-solver/src")
@@ -256,3 +257,53 @@ def time_reference(nx, ny, nz, nsteps, warmup=0, omega=1.9, ubulk=0.05, procs=No
     slowest = max(secs)
     cells = float(slab) * ny * nz * nsteps * procs
     return cells / slowest / 1e6, slowest, procs, slab
+
+
+# ---------------------------------------------------------------- quadrant analysis
+def quadrant(vel):
+    """quadrant-analysis/src/qUADrantA.c:40-170 restated (numpy, FP64): per
+    wall-normal plane k = 1..zd-2 the plane means of u, w over (x, y); the
+    fluctuations u' = u - <u>, w' = w - <w>; the four quadrants Q1 (u'>0,
+    w'>0), Q2 (u'<0, w'>0), Q3 (u'<0, w'<0), Q4 (u'>0, w'<0) (a zero u' or
+    w' falls in none).  Returns quadrant[4][zd] (conditional means of u'w'),
+    dquadrant[4][zd] (sums / cells of the plane) and uw[zd] (plane mean of
+    u'w'); wall planes 0.  vel: [nx][ny][zd][3] (vel_print.c layout)."""
+    nx, ny, zd, _ = vel.shape
+    n = nx * ny
+    q = np.zeros((4, zd))
+    dq = np.zeros((4, zd))
+    uw = np.zeros(zd)
+    for k in range(1, zd - 1):
+        u = vel[:, :, k, 0]
+        w = vel[:, :, k, 2]
+        up = u - u.sum() / n
+        wp = w - w.sum() / n
+        p = up * wp
+        uw[k] = p.sum() / n
+        masks = ((up > 0) & (wp > 0), (up < 0) & (wp > 0), (up < 0) & (wp < 0), (up > 0) & (wp < 0))
+        for a, m in enumerate(masks):
+            s_ = p[m].sum()
+            with np.errstate(invalid="ignore", divide="ignore"):
+                q[a, k] = s_ / m.sum()
+            dq[a, k] = s_ / n
+    return q, dq, uw
+
+
+def have_quadrant_reference() -> bool:
+    return os.path.exists(QUAD_BIN)
+
+
+def quadrant_reference(vel, label=0, timeout=300):
+    """The reference's own qUADrantA (oracle/_ref/quadref) on one velocity
+    field; returns (quadrant[4][zd], dquadrant[4][zd], uw[zd]) as it writes
+    them (quadrant.000.TTTT: [4][zd] then [zd])."""
+    if not have_quadrant_reference():
+        raise FileNotFoundError(QUAD_BIN)
+    nx, ny, zd, _ = vel.shape
+    with tempfile.TemporaryDirectory() as td:
+        np.ascontiguousarray(vel, np.float64).tofile(os.path.join(td, "vel.bin"))
+        subprocess.run([QUAD_BIN, str(nx), str(ny), str(zd - 2), "vel.bin", str(label)], cwd=td, check=True,
+                       timeout=timeout, stdout=subprocess.DEVNULL)
+        a = np.fromfile(os.path.join(td, f"quadrant.000.{label:04d}"))
+        b = np.fromfile(os.path.join(td, f"dquadrant.000.{label:04d}"))
+    return a[:4 * zd].reshape(4, zd), b[:4 * zd].reshape(4, zd), a[4 * zd:]

@@ -31,6 +31,13 @@ CASES = [
 ]
 
 
+# quadrant-analysis cases: name, (nx, ny, nz), steps of the oracle, seed
+QUADRANT_CASES = [
+    ("quadrant_16x12x10", (16, 12, 10), 9, 11),
+    ("quadrant_33x20x14", (33, 20, 14), 6, 12),
+]
+
+
 def case_input(nx, ny, nz, seed):
     # perturbed Poiseuille at equilibrium, +-10% of u_max on every component
     return inputs.laminar_state(nx, ny, nz, 0.08, 0.1, seed)
@@ -48,6 +55,16 @@ def main():
             seed=seed, state=r["state"], force=r["force"], rho=r["rho"],
             logs=np.stack([r[n] for n in ("energy", "flowrate", "massrate", "stup", "stdown", "stress", "pgrad")], 1),
             stats_first=r["stats"][0], stats_last=r["stats"][-1], vel_last=r["vel"][-1], den_last=r["den"][-1])
+        print(name, "ok")
+    # quadrant analysis (quadrant-analysis/src/qUADrantA.c) of the velocity
+    # field of a stepped channel, through the reference's own function
+    for name, (nx, ny, nz), steps, seed in QUADRANT_CASES:
+        st = inputs.laminar_state(nx, ny, nz, 0.08, 0.3, seed)
+        oracle.run(st, inputs.flags_smooth(nx, ny, nz), 1.7, gx=2e-5, const_g=True, nsteps=steps)
+        vel, _ = oracle.moments(st)
+        q, dq, uw = oracle.quadrant_reference(vel, label=7)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), dims=np.array([nx, ny, nz]), steps=steps,
+                            seed=seed, quadrant=q, dquadrant=dq, uw=uw)
         print(name, "ok")
 
 

@@ -44,19 +44,21 @@ def _run(nx, ny, nz, tex, steps, seg=None, const_g=True):
 @pytest.mark.parametrize("steps", [7, 8])
 @pytest.mark.parametrize("tex", ["smooth", "ridges"])
 def test_long_fp64_rows_are_segmented_and_exact(oracle_mod, tex, steps):
-    kernel, s0, fl, got, _ = _run(1256, 18, 14, tex, steps)
+    kernel, s0, fl, got, logs = _run(1256, 18, 14, tex, steps)
     assert "x-segments" in kernel, kernel
-    oracle_mod.run(s0, fl, 1.8, gx=2e-5, const_g=True, nsteps=steps)
+    ref_logs = oracle_mod.run(s0, fl, 1.8, gx=2e-5, const_g=True, nsteps=steps)
     np.testing.assert_array_equal(got, s0)
+    np.testing.assert_allclose(logs[:, 1:], ref_logs[:, 1:], rtol=1e-10, atol=1e-15)
 
 
 @pytest.mark.parametrize("nx,seg", [(100, 34), (101, 34), (64, 16)])
 @pytest.mark.parametrize("tex", ["smooth", "ridges"])
 def test_forced_segments_are_exact(oracle_mod, nx, seg, tex):
-    kernel, s0, fl, got, _ = _run(nx, 12, 9, tex, 9, seg=seg)
+    kernel, s0, fl, got, logs = _run(nx, 12, 9, tex, 9, seg=seg)
     assert "x-segments" in kernel, kernel
-    oracle_mod.run(s0, fl, 1.8, gx=2e-5, const_g=True, nsteps=9)
+    ref_logs = oracle_mod.run(s0, fl, 1.8, gx=2e-5, const_g=True, nsteps=9)
     np.testing.assert_array_equal(got, s0)
+    np.testing.assert_allclose(logs[:, 1:], ref_logs[:, 1:], rtol=1e-10, atol=1e-15)
 
 
 def test_segments_constant_q(oracle_mod):
