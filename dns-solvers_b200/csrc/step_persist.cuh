@@ -350,10 +350,10 @@ __device__ __forceinline__ bool persist_grid_barrier(const PersistArgs &a, unsig
     return s_go != 0;
 }
 
-// ANYQ: some channel runs with a constant flow rate (the launch bounds of
-// TmaBounds follow it).
+// ANYQ: some channel runs with a constant flow rate; without, FP32/FP16
+// batches take the dense launch bounds (256 threads, 2 blocks per SM).
 template <typename T, bool ANYQ>
-__global__ void __launch_bounds__(TmaBounds<T, ANYQ>::threads, TmaBounds<T, ANYQ>::blocks)
+__global__ void __launch_bounds__(TmaBounds<T, ANYQ>::threads, TmaBounds<T, ANYQ>::has_dense ? 2 : 1)
     persist_batch_kernel(const PersistArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];

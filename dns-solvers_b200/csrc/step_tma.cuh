@@ -649,17 +649,18 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
 
 constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer warp
 
-// Launch bounds of the row-pipelined kernels.  The FP32/FP16 constant-force
-// step fits 128 registers without spilling, so it is compiled for up to 256
-// threads and two blocks per SM (more warps in flight to hide the latency of
-// its dependency chains); the FP64 step and the constant-Q steps keep up to
-// 168 registers and 384 threads.
+// Launch bounds of the row-pipelined kernels.  Every step is compiled
+// "wide": up to 384 threads (11 consumer warps), one block per SM, up to 168
+// registers.  The FP32/FP16 constant-force step, which fits 128 registers
+// without spilling, is also compiled "dense": up to 256 threads and two
+// blocks per SM (more warps in flight where the stages are small enough for
+// two blocks).  A launch of more than 256 threads takes the wide form.
 template <typename T, bool CONSTQ>
 struct TmaBounds {
-    static constexpr bool wide = std::is_same<T, double>::value || CONSTQ;
-    static constexpr int threads = wide ? kTmaMaxThreads : 256;
-    static constexpr int blocks = wide ? 1 : 2;
+    static constexpr bool has_dense = !std::is_same<T, double>::value && !CONSTQ;
+    static constexpr int threads = has_dense ? 256 : kTmaMaxThreads;  // the dense form, when there is one
 };
+constexpr int kTmaDenseThreads = 256;
 
 // The consumers' work on one row group in a stage: FP64 one cell per thread
 // and iteration in the reference's operand order; FP32/FP16 cell pairs on
@@ -763,12 +764,19 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
     }
 }
 
-template <typename T, bool ODD, bool CONSTQ, int TEX>
-__global__ void __launch_bounds__(TmaBounds<T, CONSTQ>::threads, TmaBounds<T, CONSTQ>::blocks)
+template <typename T, bool ODD, bool CONSTQ, int TEX, bool WIDE>
+__global__ void __launch_bounds__(WIDE ? kTmaMaxThreads : kTmaDenseThreads, WIDE ? 1 : 2)
     step_tma_kernel(const StepArgs p, const TmaArgs t)
 {
     extern __shared__ __align__(128) unsigned char tma_smem[];
-    tma_step_body<T, ODD, CONSTQ, TEX>(p, t, blockIdx.x, tma_smem);
+    if constexpr (WIDE || TmaBounds<T, CONSTQ>::has_dense) tma_step_body<T, ODD, CONSTQ, TEX>(p, t, blockIdx.x, tma_smem);
+}
+
+// the form of step_tma_kernel a launch of `threads` threads takes
+template <typename T, bool CONSTQ>
+__host__ __forceinline__ bool tma_wide(int threads)
+{
+    return !TmaBounds<T, CONSTQ>::has_dense || threads > kTmaDenseThreads;
 }
 
 // Many independent channels in one launch: block b belongs to the channel c
@@ -815,12 +823,16 @@ template <typename T>
 int tma_set_smem_attr(size_t bytes)
 {
     const void *ks[] = {
-        (const void *)step_tma_kernel<T, false, false, 0>, (const void *)step_tma_kernel<T, false, false, 1>,
-        (const void *)step_tma_kernel<T, false, true, 0>,  (const void *)step_tma_kernel<T, false, true, 1>,
-        (const void *)step_tma_kernel<T, true, false, 0>,  (const void *)step_tma_kernel<T, true, false, 1>,
-        (const void *)step_tma_kernel<T, true, true, 0>,   (const void *)step_tma_kernel<T, true, true, 1>};
-    for (const void *k : ks)
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) return -1;
+        (const void *)step_tma_kernel<T, false, false, 0, true>, (const void *)step_tma_kernel<T, false, false, 1, true>,
+        (const void *)step_tma_kernel<T, false, true, 0, true>,  (const void *)step_tma_kernel<T, false, true, 1, true>,
+        (const void *)step_tma_kernel<T, true, false, 0, true>,  (const void *)step_tma_kernel<T, true, false, 1, true>,
+        (const void *)step_tma_kernel<T, true, true, 0, true>,   (const void *)step_tma_kernel<T, true, true, 1, true>,
+        (const void *)step_tma_kernel<T, false, false, 0, false>, (const void *)step_tma_kernel<T, false, false, 1, false>,
+        (const void *)step_tma_kernel<T, true, false, 0, false>,  (const void *)step_tma_kernel<T, true, false, 1, false>};
+    const int n = TmaBounds<T, false>::has_dense ? 12 : 8;
+    for (int i = 0; i < n; ++i)
+        if (cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+            return -1;
     return 0;
 }
 
@@ -828,10 +840,12 @@ template <typename T>
 int tma_occupancy(int threads, size_t smem, bool const_q)
 {
     int n = 0;
-    if (threads > (const_q ? TmaBounds<T, true>::threads : TmaBounds<T, false>::threads)) return 0;
-    const cudaError_t e =
-        const_q ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, true, 0>, threads, smem)
-                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0>, threads, smem);
+    if (threads > kTmaMaxThreads) return 0;
+    cudaError_t e;
+    if (const_q) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, true, 0, true>, threads, smem);
+    else if (tma_wide<T, false>(threads))
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0, true>, threads, smem);
+    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0, false>, threads, smem);
     return e == cudaSuccess ? n : 0;
 }
 
@@ -840,7 +854,12 @@ void launch_tma(const StepArgs &p, const TmaArgs &t, int grid, int threads, size
                 cudaStream_t s)
 {
     const bool q = p.const_q != 0;
-#define L(O, C, X) step_tma_kernel<T, O, C, X><<<grid, threads, smem, s>>>(p, t)
+    const bool wide = q ? tma_wide<T, true>(threads) : tma_wide<T, false>(threads);
+#define L(O, C, X)                                                                            \
+    do {                                                                                      \
+        if (wide || !TmaBounds<T, C>::has_dense) step_tma_kernel<T, O, C, X, true><<<grid, threads, smem, s>>>(p, t); \
+        else step_tma_kernel<T, O, C, X, false><<<grid, threads, smem, s>>>(p, t);           \
+    } while (0)
 #define LX(O, C) do { if (tex) L(O, C, 1); else L(O, C, 0); } while (0)
     if (odd) {
         if (q) LX(true, true); else LX(true, false);

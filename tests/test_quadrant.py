@@ -64,18 +64,23 @@ def test_gpu_quadrant_of_the_live_state(oracle_mod, path):
 
 @pytest.mark.gpu
 def test_run_dns_writes_quadrant_files(oracle_mod, tmp_path):
+    """run-dns -p from a perturbed field with QUADRANT 1: the quadrant files
+    of every output event against the restatement on that event's vel file."""
     d = str(tmp_path)
+    nx, ny, nz = 16, 8, 6
     with open(os.path.join(d, "deck.txt"), "w") as f:
-        f.write("xdv 16\nydv 8\nzdv 6\nRebs 100\nub 0.1\nCFL 0.1\nTSTR 0\nTEND 5\nITER 61\nQUADRANT 1\n"
-                "FORCE g\nGX 2e-5\n")
-    subprocess.run([RUN_DNS, "-s", "deck.txt"], cwd=d, check=True, timeout=120, capture_output=True)
-    zd = 8
-    for label in (0, 1, 2):
-        vel = np.fromfile(os.path.join(d, f"vel.{label:04d}")).reshape(16, 8, zd, 3)
+        f.write(f"xdv {nx}\nydv {ny}\nzdv {nz}\nRebs 100\nub 0.1\nCFL 0.1\nTSTR 4\nTEND 9\nITER 61\n"
+                "QUADRANT 1\nFORCE g\nGX 2e-5\n")
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.3, 9)
+    np.concatenate([s0.ravel(), s0.ravel()]).tofile(os.path.join(d, "lbf.0004"))
+    subprocess.run([RUN_DNS, "-p", "deck.txt"], cwd=d, check=True, timeout=120, capture_output=True)
+    zd = nz + 2
+    for label in (4, 5, 6):
+        vel = np.fromfile(os.path.join(d, f"vel.{label:04d}")).reshape(nx, ny, zd, 3)
         q, dq, uw = oracle_mod.quadrant(vel)
         a = np.fromfile(os.path.join(d, f"quadrant.000.{label:04d}"))
         b = np.fromfile(os.path.join(d, f"dquadrant.000.{label:04d}"))
+        np.testing.assert_allclose(a[:4 * zd].reshape(4, zd), q, rtol=1e-9, atol=1e-20)
         np.testing.assert_allclose(b[:4 * zd].reshape(4, zd), dq, rtol=1e-10, atol=1e-20)
         np.testing.assert_allclose(a[4 * zd:], uw, rtol=1e-10, atol=1e-20)
-        if label:  # the rest state at label 0 has no fluctuations: 0/0 in every quadrant, as the reference
-            np.testing.assert_allclose(a[:4 * zd].reshape(4, zd), q, rtol=1e-9, atol=1e-20)
+        np.testing.assert_array_equal(a[4 * zd:], b[4 * zd:])
