@@ -1351,7 +1351,7 @@ extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t re
         double ms = 1e30;
         TmaChoice ch{};
         int k = -1, st = -1, seg = 0, cons = 0;
-    } be, bo;  // best even / odd step shape
+    } be, bo, bt;  // best even / odd step shape, best shape for both
     auto timed = [&](int k, int st, int seg, int cons) -> int {
         double ms, e, o;
         int r = time_choice(c, steps, &ms, &e, &o);
@@ -1359,13 +1359,20 @@ extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t re
         ++ncand;
         if (e < be.ms) be.ms = e, be.ch = save_choice(c), be.k = k, be.st = st, be.seg = seg, be.cons = cons;
         if (o < bo.ms) bo.ms = o, bo.ch = save_choice(c), bo.k = k, bo.st = st, bo.seg = seg, bo.cons = cons;
+        if (ms < bt.ms) bt.ms = ms, bt.ch = save_choice(c), bt.k = k, bt.st = st, bt.seg = seg, bt.cons = cons;
         return DNSLBM_OK;
     };
+    // the default consumer count and the widest consumer sets (a block with
+    // large stages is alone on its SM and needs more warps)
+    const int widest = std::min(352, (c->nx + 31) / 32 * 32 + 32);
     for (int k : {1, 2, 4, 8})
-        for (int st : {2, 3, 4}) {
-            if (k > c->ny || tma_configure(c, k, st, cons0, 0)) continue;
-            if ((rc = timed(k, st, 0, cons0))) return rc;
-        }
+        for (int st : {2, 3, 4})
+            for (int cons : {cons0, 224, widest}) {
+                if ((cons != cons0 && (cons <= cons0 || (cons == 224 && widest <= 224))) || k > c->ny ||
+                    tma_configure(c, k, st, cons, 0))
+                    continue;
+                if ((rc = timed(k, st, 0, cons))) return rc;
+            }
     // FP64 rows as x-segments (the only bulk-copy form for rows too long for
     // two whole-row stages)
     if (c->deck.precision == 64 && c->nx >= 256)
@@ -1376,30 +1383,38 @@ extern "C" int dnslbm_autotune(dnslbm_ctx *c, int steps, char *report, size_t re
                 if ((rc = timed(1, st, seg, cons0))) return rc;
             }
     // consumer counts, then a cap on the blocks per SM, for each parity's best
-    for (int pass = 0; pass < 2; ++pass) {
-        const Best b0 = pass == 0 ? be : bo;
-        if (b0.k < 0 || (pass == 1 && bo.k == be.k && bo.st == be.st && bo.seg == be.seg)) continue;
-        for (int cons = 64; cons <= 352 && cons <= (c->nx + 31) / 32 * 32 + 32; cons += 32) {
-            if (cons == cons0 || tma_configure(c, b0.k, b0.st, cons, 0, b0.seg)) continue;
+    const Best leaders[3] = {be, bo, bt};
+    for (int pass = 0; pass < 3; ++pass) {
+        const Best b0 = leaders[pass];
+        bool seen = false;
+        for (int q = 0; q < pass; ++q)
+            seen |= leaders[q].k == b0.k && leaders[q].st == b0.st && leaders[q].seg == b0.seg;
+        if (b0.k < 0 || seen) continue;
+        for (int cons = 64; cons <= widest; cons += 32) {
+            if (cons == cons0 || cons == 224 || cons == widest || tma_configure(c, b0.k, b0.st, cons, 0, b0.seg)) continue;
             if ((rc = timed(b0.k, b0.st, b0.seg, cons))) return rc;
         }
     }
-    for (int pass = 0; pass < 2; ++pass) {
-        const Best b0 = pass == 0 ? be : bo;
+    const Best leaders2[3] = {be, bo, bt};
+    for (int pass = 0; pass < 3; ++pass) {
+        const Best b0 = leaders2[pass];
         if (b0.k < 0) continue;
         for (int bps : {1, 2, 3}) {
             if (tma_configure(c, b0.k, b0.st, b0.cons, bps, b0.seg)) continue;
             if ((rc = timed(b0.k, b0.st, b0.seg, b0.cons))) return rc;
         }
     }
+    if (bt.k > 0 && bt.ms < best_ms) best_ms = bt.ms, best = bt.ch;  // one shape for both parities
     if (be.k > 0) {
         const bool same = be.ch.threads == bo.ch.threads && be.ch.grid == bo.ch.grid && be.ch.smem == bo.ch.smem &&
                           be.ch.t.k == bo.ch.t.k && be.ch.t.stages == bo.ch.t.stages && be.ch.t.nseg == bo.ch.t.nseg;
-        load_choice(c, same ? be.ch : split_choice(be.ch, bo.ch));
-        double ms;
-        if ((rc = time_choice(c, steps, &ms))) return rc;  // the combination, measured
-        ++ncand;
-        if (ms < best_ms) best_ms = ms, best = save_choice(c);
+        if (!same) {  // the parities' own shapes, measured together (a change of shape between launches costs too)
+            load_choice(c, split_choice(be.ch, bo.ch));
+            double ms;
+            if ((rc = time_choice(c, steps, &ms))) return rc;
+            ++ncand;
+            if (ms < best_ms) best_ms = ms, best = save_choice(c);
+        }
     }
     load_choice(c, best);
     describe_kernel(c);

@@ -56,16 +56,15 @@ struct PersistArgs {
 };
 
 // Per-stage header, written by the producer before it arms the stage: the
-// channel's arguments and the item and row group of the stage, so the
-// consumers find their work without a global-memory round trip.
+// item and row group of the stage.  The channel's arguments stay in the
+// read-only global table (a restrict pointer lets the compiler keep them in
+// registers across the consumers' shared-memory stores; a copy in shared
+// memory would be reloaded after each of them).
 struct StageHeader {
-    ChannelLaunch L;  // the item's channel (copied when the stage held another)
     BatchItem it;
-    int item;         // index of the item; -1 ends the step
-    int group;        // row group within the item; -1 for a kind-1 item
-    int z, y0;        // plane and first row of the group (kind 1: plane, unused)
-    int chan;         // channel whose arguments L holds
-    int pad_;
+    int item;   // index of the item; -1 ends the step
+    int group;  // row group within the item; -1 for a kind-1 item
+    int z, y0;  // plane and first row of the group (kind 1: plane, unused)
 };
 
 // Shared memory after the stages: full[S], empty[S] (8 bytes each), then
@@ -105,6 +104,7 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
                                                  volatile int *s_abort)
 {
     const int S = a.stages;
+    const ChannelLaunch *__restrict__ chans = a.chans;
     int i = 0;            // stage sequence number within the step
     // test switch: the block that takes the first item of the first step
     // neither arms nor loads its first row group, so its consumers' wait runs
@@ -119,7 +119,7 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
             persist_raise(a, s_abort);
         const StageHeader &H = hdr[st];
         if (*s_abort || H.item < 0 || H.group < 0 || lane >= Q) return;
-        const ChannelLaunch &L = H.L;
+        const ChannelLaunch &L = chans[H.it.chan];
         const int k = min(L.t.k, L.p.ny - H.y0);
         const int wall = H.z == 0 ? -1 : (H.z == L.p.nz - 1 ? 1 : 0);
         const GroupRows gr = L.textured ? group_rows<ODD, 1>(L.p, lane, H.y0, H.z, wall)
@@ -135,23 +135,15 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
         __syncwarp();
         return i % S;
     };
-    // the header of a stage: the channel's arguments (when the stage held
-    // another channel) and the item's per-step values
+    // the header of a stage: the item and the row group it holds
     auto fill = [&](int st, int h, const BatchItem &it, int g, int z, int y0) {
-        StageHeader &H = hdr[st];
-        const int had = __shfl_sync(0xffffffffu, lane == 0 ? H.chan : 0, 0);
-        if (had != it.chan) {
-            const int *src = reinterpret_cast<const int *>(a.chans + it.chan);
-            int *dst = reinterpret_cast<int *>(&H.L);
-            for (int w = lane; w < (int)(sizeof(ChannelLaunch) / sizeof(int)); w += 32) dst[w] = __ldg(src + w);
-        }
         if (lane == 0) {
+            StageHeader &H = hdr[st];
             H.it = it;
             H.item = h;
             H.group = g;
             H.z = z;
             H.y0 = y0;
-            H.chan = it.chan;
         }
         __syncwarp();
     };
@@ -167,7 +159,7 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
             __syncwarp();
             ++i;
         } else {
-            const ChannelLaunch &L = a.chans[it.chan];
+            const ChannelLaunch &L = chans[it.chan];
             const size_t dir_bytes = (size_t)L.t.dir_elems * sizeof(T);
             for (int g = 0; g < it.count; ++g) {
                 const int st = next_stage();
@@ -242,6 +234,7 @@ __device__ __forceinline__ void persist_consumers(const PersistArgs &a, int s, u
 {
     using LpT = typename std::conditional<std::is_same<T, double>::value, float, T>::type;
     const int S = a.stages;
+    const ChannelLaunch *__restrict__ chans = a.chans;
     // parity of the step counter (every channel of a batch is at the same
     // step, and a loaded state starts at step 0 with the even AA step)
     const int sp = (a.first_odd + s) & 1;
@@ -261,7 +254,8 @@ __device__ __forceinline__ void persist_consumers(const PersistArgs &a, int s, u
         }
         const StageHeader &H = hdr[st];
         if (H.item < 0) return;  // end of the step (the same header for every consumer)
-        const StepArgs &p = H.L.p;
+        const ChannelLaunch &L = chans[H.it.chan];
+        const StepArgs &p = L.p;
         const bool q = ANYQ && p.const_q != 0;  // a batch without constant-Q channels compiles no such path
         const int z = H.z;
         if (H.group <= 0) {  // an item's first stage
@@ -275,15 +269,15 @@ __device__ __forceinline__ void persist_consumers(const PersistArgs &a, int s, u
             if (q) persist_links<T, ODD, true>(p, H.it, G, sh, acc, nc);
             else persist_links<T, ODD, false>(p, H.it, G, sh, acc, nc);
         } else {
-            const int k = min(H.L.t.k, p.ny - H.y0);
-            const int dstride = H.L.t.dir_elems;
+            const int k = min(L.t.k, p.ny - H.y0);
+            const int dstride = L.t.dir_elems;
             T *sb = reinterpret_cast<T *>(smem + (size_t)st * a.stage_bytes);
             [[maybe_unused]] const LpParams lk = lp_params<LpT>((float)p.omega, (float)G);
             if (q) {
-                if (H.L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
+                if (L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
                 else consume_group<T, ODD, true, false>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
             } else {
-                if (H.L.textured) consume_group<T, ODD, false, true>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
+                if (L.textured) consume_group<T, ODD, false, true>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
                 else consume_group<T, ODD, false, false>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
             }
             fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
@@ -311,7 +305,6 @@ __device__ __forceinline__ void persist_step(const PersistArgs &a, int s, unsign
         for (int st = 0; st < S; ++st) {
             mbar_init(full + st, 1);
             mbar_init(empty + st, nc / 32);
-            hdr[st].chan = -1;  // no channel arguments copied yet
         }
         fence_mbar_init();
     }

@@ -780,8 +780,9 @@ __host__ __forceinline__ bool tma_wide(int threads)
 }
 
 // Many independent channels in one launch: block b belongs to the channel c
-// with first[c] <= b < first[c+1]; the channel's arguments are copied to
-// shared memory and the block runs that channel's step.
+// with first[c] <= b < first[c+1] and runs that channel's step, reading its
+// arguments from the read-only table (through a restrict pointer, so they
+// stay in registers across the block's shared-memory stores).
 struct ChannelLaunch {
     StepArgs p;
     TmaArgs t;
@@ -794,20 +795,9 @@ __global__ void __launch_bounds__(kTmaMaxThreads, 1) step_tma_batch_kernel(const
                                                                            int nchan)
 {
     extern __shared__ __align__(128) unsigned char tma_smem[];
-    __shared__ ChannelLaunch L;
-    __shared__ int s_c;
-    if (threadIdx.x == 0) {
-        int c = 0;
-        while (c + 1 < nchan && chans[c + 1].first_block <= (int)blockIdx.x) ++c;
-        s_c = c;
-    }
-    __syncthreads();
-    {
-        const int *src = reinterpret_cast<const int *>(chans + s_c);
-        int *dst = reinterpret_cast<int *>(&L);
-        for (int i = threadIdx.x; i < (int)(sizeof(ChannelLaunch) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
-    }
-    __syncthreads();
+    int c = 0;
+    while (c + 1 < nchan && chans[c + 1].first_block <= (int)blockIdx.x) ++c;
+    const ChannelLaunch &L = chans[c];
     const int blk = blockIdx.x - L.first_block;
     const bool q = L.p.const_q != 0;
     if (q) {
