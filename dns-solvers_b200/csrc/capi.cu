@@ -1570,11 +1570,12 @@ static void batch_layout(dnslbm_batch *b)
 }
 
 // The items of one step of the persistent kernel: each plane of each
-// channel cut into runs of whole row groups (planes without link masks) or
-// of rows (planes with them) of about W cells, W chosen so that every
-// resident block takes about four items per step; largest first, so the
-// last items taken are the small ones.  An item's slot is its index within
-// its plane, so the plane sums do not depend on which block takes it.
+// channel cut into runs of whole row groups of about W cells, W chosen so
+// that every resident block takes about four items per step; kind 1 for the
+// planes with link masks (the channel's plane list holds them after the
+// others, so the group numbering covers them).  Largest first, so the last
+// items taken are the small ones.  An item's slot is its index within its
+// plane, so the plane sums do not depend on which block takes it.
 static void persist_items(dnslbm_batch *b)
 {
     double total = 0;
@@ -1585,7 +1586,7 @@ static void persist_items(dnslbm_batch *b)
     for (int ci = 0; ci < (int)b->ch.size(); ++ci) {
         dnslbm_ctx *c = b->ch[ci];
         const TmaArgs &t = c->tma;
-        for (int pi = 0; pi < c->nclean; ++pi) {
+        for (int pi = 0; pi < c->nz; ++pi) {
             const double gcells = (double)t.k * c->nx;
             const int per = std::max(1, (int)(W / gcells));
             const int n = (t.gpp + per - 1) / per;
@@ -1593,7 +1594,7 @@ static void persist_items(dnslbm_batch *b)
                 const int g0 = (int)((long long)t.gpp * j / n), g1 = (int)((long long)t.gpp * (j + 1) / n);
                 BatchItem x{};
                 x.chan = ci;
-                x.kind = 0;
+                x.kind = pi < c->nclean ? 0 : 1;
                 x.first = pi * t.gpp + g0;
                 x.count = g1 - g0;
                 x.plane = c->plane_host[pi];
@@ -1601,22 +1602,6 @@ static void persist_items(dnslbm_batch *b)
                 x.ncontrib = n;
                 it.push_back(x);
                 cells.push_back(std::min((double)(g1 - g0) * t.k, (double)c->ny) * c->nx);
-            }
-        }
-        for (int pi = c->nclean; pi < c->nz; ++pi) {
-            const int per = std::max(1, (int)(W / c->nx));
-            const int n = (c->ny + per - 1) / per;
-            for (int j = 0; j < n; ++j) {
-                BatchItem x{};
-                x.chan = ci;
-                x.kind = 1;
-                x.plane = c->plane_host[pi];
-                x.y0 = (int)((long long)c->ny * j / n);
-                x.y1 = (int)((long long)c->ny * (j + 1) / n);
-                x.slot = j;
-                x.ncontrib = n;
-                it.push_back(x);
-                cells.push_back((double)(x.y1 - x.y0) * c->nx);
             }
         }
     }

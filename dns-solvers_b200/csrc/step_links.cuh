@@ -132,13 +132,17 @@ __device__ __forceinline__ void solid_sums(const RegT<T> (&f)[Q], double c0, dou
 // One cell with link mask `lk` (plane `wall` = -1 bottom, +1 top, 0
 // interior).  Even step: the cell's own populations, from shared memory at
 // sbx[A * dstride] when sbx is given (the bulk-copied own rows), else from
-// global memory.  Odd step: global memory through the link addresses.
+// global memory.  Odd step: global memory through the link addresses, except
+// that with sbx given (the bulk-copied rows of the odd address set, element
+// x at sbx, x - 1 at sbx + om, x + 1 at sbx + op) a link that neither
+// bounces nor meets a wall is read from shared memory; the odd step's
+// results always go to global memory.
 // FP64 sums go to acc; low-precision sums go to racc (FP32, flushed by the
 // caller) except the cell counts, which go to acc[0] and acc[6].
 template <typename T, bool ODD, bool CONSTQ>
 __device__ __forceinline__ void links_cell(const StepArgs &p, const Nbr &n, int wall, unsigned lk, T *sbx, int dstride,
                                            double G, double c0, double c1, double c2, double (&acc)[NP],
-                                           float (&racc)[NP])
+                                           float (&racc)[NP], int om = 0, int op = 0)
 {
     using V = RegT<T>;
     if (lk & 1u) {
@@ -154,8 +158,11 @@ __device__ __forceinline__ void links_cell(const StepArgs &p, const Nbr &n, int 
     static_for<Q>([&](auto ac) {
         constexpr int A = decltype(ac)::value;
         V v;
+        constexpr int ex = lat_ex(A), ez = lat_ez(A);
         if (!ODD && sbx) v = ld_raw<T>(sbx + A * dstride);
         else if (!ODD) v = ld_glb<T>(static_cast<const T *>(p.pop[A]) + n.c0);
+        else if (sbx && !((lk >> A) & 1u) && !(ez != 0 && wall == ez))
+            v = ld_raw<T>(sbx + A * dstride + (ex > 0 ? op : (ex < 0 ? om : 0)));
         else v = ld_glb<T>(links_ptr<T, A>(p, n, wall, lk));
         f[ODD ? lat_opp(A) : A] = v;
     });

@@ -2,14 +2,21 @@
 //
 // One cooperative launch (every block resident at once) advances all
 // channels of a batch through nsteps time steps.  Within a step the work is
-// a table of items, largest first:
-//   kind 0  a run of row groups of one plane of one channel, moved through
-//           the block's shared-memory stages by the bulk-copy engine and
-//           collided by the consumer warps (the row-pipelined step of
-//           step_tma.cuh);
-//   kind 1  the cells of some rows of a plane with per-cell link masks
-//           (solids inside the flow), collided by the consumer warps from
-//           global memory (links_cell).
+// a table of items, largest first, each a run of row groups of one plane of
+// one channel moved through the block's shared-memory stages by the
+// bulk-copy engine and collided by the consumer warps:
+//   kind 0  a plane without link masks: the row-pipelined step of
+//           step_tma.cuh (rows in, rows out);
+//   kind 1  a plane with per-cell link masks (solids inside the flow), one
+//           cell per thread (links_cell).  An even step touches only the
+//           cells' own rows, which go in and out as for kind 0.  An odd step
+//           brings in the rows of the regular address set; a link that
+//           bounces back or meets a wall reads its own address from global
+//           memory, and every result goes to global memory: a bounced link's
+//           address lies in a row of another cell row's set (that of the
+//           solid neighbour, which is never collided), so the rows are not
+//           stored back.  Every address is still read and written by one
+//           cell only.
 // A block's producer warp takes the next item from the step's counter
 // (atomicAdd), so blocks that drew small items take more: no block waits
 // for a channel it owns.  Each item sums its cells into its own partial-sum
@@ -37,9 +44,8 @@ namespace dnslbm {
 struct BatchItem {
     int chan;            // index into the channel table
     int kind;            // 0: row groups through the stages, 1: cells of a plane with link masks
-    int first, count;    // kind 0: row groups first .. first+count-1 (channel's group numbering)
-    int plane;           // kind 1: the plane z
-    int y0, y1;          // kind 1: rows y0 .. y1-1
+    int first, count;    // row groups first .. first+count-1 (the channel's group numbering)
+    int plane;           // the plane z
     int slot, ncontrib;  // partial-sum slot of the item in its plane, items of that plane
 };
 
@@ -63,8 +69,8 @@ struct PersistArgs {
 struct StageHeader {
     BatchItem it;
     int item;   // index of the item; -1 ends the step
-    int group;  // row group within the item; -1 for a kind-1 item
-    int z, y0;  // plane and first row of the group (kind 1: plane, unused)
+    int group;  // row group within the item
+    int z, y0;  // plane and first row of the group
 };
 
 // Shared memory after the stages: full[S], empty[S] (8 bytes each), then
@@ -118,7 +124,8 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
         if (!*s_abort && !mbar_wait_bounded(empty + st, (uint32_t)((seq / S) & 1), a.wait_ns, s_abort))
             persist_raise(a, s_abort);
         const StageHeader &H = hdr[st];
-        if (*s_abort || H.item < 0 || H.group < 0 || lane >= Q) return;
+        // a kind-1 item's odd-step results went to global memory
+        if (*s_abort || H.item < 0 || (ODD && H.it.kind == 1) || lane >= Q) return;
         const ChannelLaunch &L = chans[H.it.chan];
         const int k = min(L.t.k, L.p.ny - H.y0);
         const int wall = H.z == 0 ? -1 : (H.z == L.p.nz - 1 ? 1 : 0);
@@ -152,14 +159,11 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
     while (h < a.nitems) {
         const BatchItem it = a.items[h];
         const int hn = take();  // the next item, fetched while this one is issued
-        if (it.kind == 1) {     // no copies: the consumers work from global memory
-            const int st = next_stage();
-            fill(st, h, it, -1, it.plane, it.y0);
-            if (lane == 0) mbar_arrive(full + st);
-            __syncwarp();
-            ++i;
-        } else {
+        {
             const ChannelLaunch &L = chans[it.chan];
+            // kind 1: the regular rows only (the wall links of an odd step
+            // read their own addresses, as for a textured wall)
+            const bool tex = L.textured || it.kind == 1;
             const size_t dir_bytes = (size_t)L.t.dir_elems * sizeof(T);
             for (int g = 0; g < it.count; ++g) {
                 const int st = next_stage();
@@ -169,8 +173,7 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
                 const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
                 GroupRows gr{};
                 if (lane < Q)
-                    gr = L.textured ? group_rows<ODD, 1>(L.p, lane, y0, z, wall)
-                                    : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
+                    gr = tex ? group_rows<ODD, 1>(L.p, lane, y0, z, wall) : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
                 const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && gr.bulk);
                 const bool issue = __shfl_sync(0xffffffffu, *s_abort, 0) == 0 && !(withhold_step && h == 0 && g == 0);
                 if (issue) {
@@ -205,23 +208,24 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
             if ((loaded >> st) & 1u) mbar_wait_bounded(full + st, (phase >> st) & 1u, a.wait_ns, nullptr);
 }
 
-// Kind-1 item: the cells of rows y0..y1-1 of a plane with link masks, one
-// thread per cell.
+// A row group of a kind-1 item from the stage: rows y0 .. y0+k-1 of plane z,
+// one cell per thread (links_cell; the odd step's shifted elements at x-1
+// and x+1 wrap around the row).
 template <typename T, bool ODD, bool CONSTQ>
-__device__ __forceinline__ void persist_links(const StepArgs &p, const BatchItem &it, double G, const double (&sh)[3],
-                                              double (&acc)[NP], int nc)
+__device__ __forceinline__ void persist_links(const StepArgs &p, T *sb, int dstride, int y0, int k, int z, double G,
+                                              const double (&sh)[3], double (&acc)[NP], int nc)
 {
-    const int z = it.plane, nx = p.nx;
+    const int nx = p.nx;
     const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
-    const int ncell = (it.y1 - it.y0) * nx;
-    for (int c = threadIdx.x; c < ncell; c += nc) {
-        const int dy = c / nx, x = c - dy * nx, y = it.y0 + dy;
+    for (int c = threadIdx.x; c < k * nx; c += nc) {
+        const int j = c / nx, x = c - j * nx, y = y0 + j;
         float racc[NP];
 #pragma unroll
         for (int q = 0; q < NP; ++q) racc[q] = 0.f;
         const Nbr n = make_nbr(x, y, z, nx, p.ny, p.pitch);
-        links_cell<T, ODD, CONSTQ>(p, n, wall, cell_links(p.band_of, p.links, nx, p.ny, x, y, z), nullptr, 0, G,
-                                   sh[0], sh[1], sh[2], acc, racc);
+        const int om = x == 0 ? nx - 1 : -1, op = x == nx - 1 ? 1 - nx : 1;
+        links_cell<T, ODD, CONSTQ>(p, n, wall, cell_links(p.band_of, p.links, nx, p.ny, x, y, z),
+                                   sb + (size_t)j * p.pitch + x, dstride, G, sh[0], sh[1], sh[2], acc, racc, om, op);
 #pragma unroll
         for (int q = 0; q < NP; ++q) acc[q] += (double)racc[q];
     }
@@ -258,20 +262,21 @@ __device__ __forceinline__ void persist_consumers(const PersistArgs &a, int s, u
         const StepArgs &p = L.p;
         const bool q = ANYQ && p.const_q != 0;  // a batch without constant-Q channels compiles no such path
         const int z = H.z;
-        if (H.group <= 0) {  // an item's first stage
+        if (H.group == 0) {  // an item's first stage
             G = q ? __ldcg(p.force + sp) : p.gx;
             const double *shp = p.shift + (size_t)sp * p.nz * 3 + z * 3;
             sh[0] = __ldcg(shp);
             sh[1] = __ldcg(shp + 1);
             sh[2] = __ldcg(shp + 2);
         }
-        if (H.group < 0) {
-            if (q) persist_links<T, ODD, true>(p, H.it, G, sh, acc, nc);
-            else persist_links<T, ODD, false>(p, H.it, G, sh, acc, nc);
+        const int k = min(L.t.k, p.ny - H.y0);
+        const int dstride = L.t.dir_elems;
+        T *sb = reinterpret_cast<T *>(smem + (size_t)st * a.stage_bytes);
+        if (H.it.kind == 1) {
+            if (q) persist_links<T, ODD, true>(p, sb, dstride, H.y0, k, z, G, sh, acc, nc);
+            else persist_links<T, ODD, false>(p, sb, dstride, H.y0, k, z, G, sh, acc, nc);
+            fence_async_smem();  // the even step's rows go back by bulk store
         } else {
-            const int k = min(L.t.k, p.ny - H.y0);
-            const int dstride = L.t.dir_elems;
-            T *sb = reinterpret_cast<T *>(smem + (size_t)st * a.stage_bytes);
             [[maybe_unused]] const LpParams lk = lp_params<LpT>((float)p.omega, (float)G);
             if (q) {
                 if (L.textured) consume_group<T, ODD, true, true>(p, lk, sb, dstride, H.y0, k, z, G, sh, acc, nc);
@@ -282,7 +287,7 @@ __device__ __forceinline__ void persist_consumers(const PersistArgs &a, int s, u
             }
             fence_async_smem();  // this thread's shared-memory writes -> visible to the bulk stores
         }
-        const bool done = H.group < 0 || H.group == H.it.count - 1;
+        const bool done = H.group == H.it.count - 1;
         if (done) {  // the item is done: its plane contribution (the stage is released after it)
             // step -1: the channel's step tail reads its own step counter
             plane_contribute(p, acc, z, H.it.slot, H.it.ncontrib, -1, G, 0, nc);
@@ -343,10 +348,11 @@ __device__ __forceinline__ bool persist_grid_barrier(const PersistArgs &a, unsig
     return s_go != 0;
 }
 
-// ANYQ: some channel runs with a constant flow rate; without, FP32/FP16
-// batches take the dense launch bounds (256 threads, 2 blocks per SM).
+// ANYQ: some channel runs with a constant flow rate.  The launch bounds are
+// those of the 256-thread step form where the precision has one (FP32
+// without ANYQ: two blocks per SM; FP16: one block, no spills).
 template <typename T, bool ANYQ>
-__global__ void __launch_bounds__(TmaBounds<T, ANYQ>::threads, TmaBounds<T, ANYQ>::has_dense ? 2 : 1)
+__global__ void __launch_bounds__(TmaBounds<T, ANYQ>::threads, TmaBounds<T, ANYQ>::min_blocks)
     persist_batch_kernel(const PersistArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];

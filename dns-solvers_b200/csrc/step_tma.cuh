@@ -651,14 +651,21 @@ constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer w
 
 // Launch bounds of the row-pipelined kernels.  Every step is compiled
 // "wide": up to 384 threads (11 consumer warps), one block per SM, up to 168
-// registers.  The FP32/FP16 constant-force step, which fits 128 registers
-// without spilling, is also compiled "dense": up to 256 threads and two
-// blocks per SM (more warps in flight where the stages are small enough for
-// two blocks).  A launch of more than 256 threads takes the wide form.
+// registers (a sub-partition's 16K registers shared by three warps).  The
+// low-precision steps are also compiled for up to 256 threads (two warps per
+// sub-partition): the FP32 constant-force step, which fits 128 registers
+// without spilling, for two blocks per SM (more warps in flight where the
+// stages are small enough for two blocks); the FP16 steps for one block per
+// SM and up to 255 registers (their cell pairs need about 190: no spills).
+// A launch of more than 256 threads takes the wide form.
 template <typename T, bool CONSTQ>
 struct TmaBounds {
-    static constexpr bool has_dense = !std::is_same<T, double>::value && !CONSTQ;
-    static constexpr int threads = has_dense ? 256 : kTmaMaxThreads;  // the dense form, when there is one
+    // blocks per SM of the 256-thread form (0: not compiled)
+    static constexpr int dense_blocks =
+        std::is_same<T, double>::value ? 0 : (std::is_same<T, __half>::value ? 1 : (CONSTQ ? 0 : 2));
+    static constexpr bool has_dense = dense_blocks > 0;
+    static constexpr int threads = has_dense ? 256 : kTmaMaxThreads;  // the 256-thread form, when there is one
+    static constexpr int min_blocks = has_dense ? dense_blocks : 1;
 };
 constexpr int kTmaDenseThreads = 256;
 
@@ -765,7 +772,7 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
 }
 
 template <typename T, bool ODD, bool CONSTQ, int TEX, bool WIDE>
-__global__ void __launch_bounds__(WIDE ? kTmaMaxThreads : kTmaDenseThreads, WIDE ? 1 : 2)
+__global__ void __launch_bounds__(WIDE ? kTmaMaxThreads : kTmaDenseThreads, WIDE ? 1 : TmaBounds<T, CONSTQ>::min_blocks)
     step_tma_kernel(const StepArgs p, const TmaArgs t)
 {
     extern __shared__ __align__(128) unsigned char tma_smem[];
@@ -818,9 +825,10 @@ int tma_set_smem_attr(size_t bytes)
         (const void *)step_tma_kernel<T, true, false, 0, true>,  (const void *)step_tma_kernel<T, true, false, 1, true>,
         (const void *)step_tma_kernel<T, true, true, 0, true>,   (const void *)step_tma_kernel<T, true, true, 1, true>,
         (const void *)step_tma_kernel<T, false, false, 0, false>, (const void *)step_tma_kernel<T, false, false, 1, false>,
-        (const void *)step_tma_kernel<T, true, false, 0, false>,  (const void *)step_tma_kernel<T, true, false, 1, false>};
-    const int n = TmaBounds<T, false>::has_dense ? 12 : 8;
-    for (int i = 0; i < n; ++i)
+        (const void *)step_tma_kernel<T, true, false, 0, false>,  (const void *)step_tma_kernel<T, true, false, 1, false>,
+        (const void *)step_tma_kernel<T, false, true, 0, false>,  (const void *)step_tma_kernel<T, false, true, 1, false>,
+        (const void *)step_tma_kernel<T, true, true, 0, false>,   (const void *)step_tma_kernel<T, true, true, 1, false>};
+    for (int i = 0; i < 16; ++i)
         if (cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
             return -1;
     return 0;
@@ -832,7 +840,10 @@ int tma_occupancy(int threads, size_t smem, bool const_q)
     int n = 0;
     if (threads > kTmaMaxThreads) return 0;
     cudaError_t e;
-    if (const_q) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, true, 0, true>, threads, smem);
+    if (const_q && tma_wide<T, true>(threads))
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, true, 0, true>, threads, smem);
+    else if (const_q)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, true, 0, false>, threads, smem);
     else if (tma_wide<T, false>(threads))
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0, true>, threads, smem);
     else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_tma_kernel<T, true, false, 0, false>, threads, smem);
