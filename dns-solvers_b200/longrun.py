@@ -95,7 +95,21 @@ def run_one(wl, s0, flags, prec, spinup, steps, sample, blocks=1, device=0):
     secs = time.perf_counter() - t0
     vel, _ = ch.moments()
     ch.close()
-    out = {"precision": prec, "seconds": round(secs, 2), "blocks": blocks}
+    out = summarize(bq, prec, secs)
+    slip = flags[:, :, 0] == -2
+    if slip.any():
+        u1 = vel[:, :, 1, 0]
+        out["slip_u_first_plane"] = float(u1[slip].mean())
+        out["noslip_u_first_plane"] = float(u1[~slip].mean())
+    return out
+
+
+def summarize(bq, prec, secs):
+    """Window averages, batch-means standard errors and folded profiles of
+    a run's block averages bq (kept under "block_values" for --save)."""
+    blocks = len(bq)
+    out = {"precision": prec, "seconds": round(secs, 2), "blocks": blocks,
+           "block_values": {k: np.array([b[k] for b in bq]) for k in bq[0]}}
     for k in bq[0]:
         vals = np.array([b[k] for b in bq])
         out[k] = vals.mean(axis=0) if vals.ndim > 1 else float(vals.mean())
@@ -105,11 +119,44 @@ def run_one(wl, s0, flags, prec, spinup, steps, sample, blocks=1, device=0):
             fv = 0.5 * (vals + vals[:, ::-1])
             out[k + "_fold"] = fv.mean(axis=0)
             out[k + "_fold_se"] = fv.std(axis=0, ddof=1) / math.sqrt(blocks) if blocks > 1 else np.zeros_like(fv[0])
-    slip = flags[:, :, 0] == -2
-    if slip.any():
-        u1 = vel[:, :, 1, 0]
-        out["slip_u_first_plane"] = float(u1[slip].mean())
-        out["noslip_u_first_plane"] = float(u1[~slip].mean())
+    return out
+
+
+def save_runs(path, runs):
+    """The block averages of every finished run, to compare later runs
+    against (--ref)."""
+    arrs = {}
+    for r in runs:
+        if "block_values" not in r:
+            continue
+        for k, v in r["block_values"].items():
+            arrs[f"{r['run']}__{k}"] = v
+        arrs[f"{r['run']}__seconds"] = np.array(r["seconds"])
+        for k in ("slip_u_first_plane", "noslip_u_first_plane"):
+            if k in r:
+                arrs[f"{r['run']}__{k}"] = np.array(r[k])
+    np.savez(path, **arrs)
+
+
+def load_runs(path):
+    """Runs saved by save_runs, by label."""
+    z = np.load(path)
+    by = {}
+    for name in z.files:
+        label, key = name.split("__", 1)
+        by.setdefault(label, {})[key] = z[name]
+    out = {}
+    for label, d in by.items():
+        secs = float(d.pop("seconds"))
+        extra = {k: float(d.pop(k)) for k in ("slip_u_first_plane", "noslip_u_first_plane") if k in d}
+        nb = len(next(iter(d.values())))
+        bq = [{k: (v[i] if v.ndim > 1 else float(v[i])) for k, v in d.items()} for i in range(nb)]
+        prec = int(label[:2])
+        r = summarize(bq, prec, secs)
+        r.update(extra)
+        r["run"] = label
+        r["from"] = os.path.basename(path)
+        out[label] = r
     return out
 
 
@@ -148,7 +195,10 @@ def main():
     ap.add_argument("--control-amp", type=float, default=1e-7, help="relative perturbation of the 64p control")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--save", default=None, help="write the runs' block averages (.npz) for a later --ref")
+    ap.add_argument("--ref", default=None, help="runs saved by --save: a listed run found there is not run again")
     a = ap.parse_args()
+    saved = load_runs(a.ref) if a.ref else {}
     wl = inputs.workload(a.workload)
     flags = inputs.make_flags(wl)
     s0 = inputs.make_state(wl, seed=a.seed)
@@ -156,6 +206,9 @@ def main():
         s0 = inputs.rest_solids(s0, flags)
     runs = []
     for p in a.precisions.split(","):
+        if p in saved:
+            runs.append(saved[p])
+            continue
         init = s0
         if p.startswith("64p"):
             amp = float(p[3:]) if len(p) > 3 else a.control_amp
@@ -177,8 +230,10 @@ def main():
         summary["note"] = ("walls with riblets: the reference's wall-stress formula (a one-sided difference of "
                            "plane means at a flat wall) does not measure the riblet drag; compare u_bulk at "
                            "the common body force")
+    if a.save:
+        save_runs(a.save, runs)
     for r in runs:
-        row = {k: v for k, v in r.items() if not isinstance(v, np.ndarray)}
+        row = {k: v for k, v in r.items() if not isinstance(v, (np.ndarray, dict))}
         if r is not ref and "failed" not in r and "failed" not in ref:
             row["error_vs_fp64"] = compare(ref, r)
         summary["runs"].append(row)
