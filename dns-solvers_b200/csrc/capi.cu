@@ -26,6 +26,10 @@ void launch_stats_sample(int nz, double np, const double *planes, double *mean, 
                          cudaStream_t s);
 void launch_stats_rows(int nz, double np, const double *mean, const double *planes, double *out, cudaStream_t s);
 void launch_quadrant(const double *vel, int nx, int ny, int zd, double *mean, double *out, cudaStream_t s);
+size_t correlation_scratch(int nx, int ny, int zd, int per_chunk);
+int correlation_max_line();
+cudaError_t launch_correlations(const double *vel, int nx, int ny, int zd, int per_chunk, double *scratch,
+                                double *xcorl, double *ycorl, double *ua, cudaStream_t s);
 int persist_prepare_f64(size_t smem);
 int persist_occupancy_f64(int threads, size_t smem, bool any_q);
 cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, bool any_q, cudaStream_t s);
@@ -1219,6 +1223,74 @@ extern "C" int dnslbm_quadrant_vel(const double *vel, int xdv, int ydv, int zdv,
     if (buf) cudaFree(buf);
     if (e != cudaSuccess) return fail(c, DNSLBM_ERR_CUDA, "quadrant analysis of a velocity field: %s", cudaGetErrorString(e));
     quadrant_finish(zd, (double)xdv * ydv, sums.data(), quadrant, dquadrant, uw);
+    return DNSLBM_OK;
+}
+
+// Two-point correlations (2pt-correlations/src: mean_subtract.c, xcorrel.c,
+// ycorrel.c) of a velocity field already in device memory: temporary device
+// memory for the fluctuations and the partial sums, results copied to the
+// caller's host arrays (any may be NULL).
+constexpr int kCorrLinesPerChunk = 8;
+
+static cudaError_t correlations_of(const double *dvel, int nx, int ny, int zd, cudaStream_t s, double *xcorl,
+                                   double *ycorl, double *uavg)
+{
+    double *scratch = nullptr, *res = nullptr;
+    const size_t nres = (size_t)zd * 3 * (nx + ny + 1);
+    cudaError_t e = cudaMalloc(&scratch, correlation_scratch(nx, ny, zd, kCorrLinesPerChunk) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&res, nres * sizeof(double));
+    double *dx = res, *dy = res + (size_t)zd * 3 * nx, *du = dy + (size_t)zd * 3 * ny;
+    if (e == cudaSuccess) e = launch_correlations(dvel, nx, ny, zd, kCorrLinesPerChunk, scratch, dx, dy, du, s);
+    std::vector<double> h(nres);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), res, nres * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (scratch) cudaFree(scratch);
+    if (res) cudaFree(res);
+    if (e != cudaSuccess) return e;
+    if (xcorl) memcpy(xcorl, h.data(), sizeof(double) * zd * 3 * nx);
+    if (ycorl) memcpy(ycorl, h.data() + (size_t)zd * 3 * nx, sizeof(double) * zd * 3 * ny);
+    if (uavg)
+        for (int k = 0; k < zd; ++k) uavg[k] = h[(size_t)zd * 3 * (nx + ny) + (size_t)k * 3];
+    return cudaSuccess;
+}
+
+extern "C" int dnslbm_correlations(dnslbm_ctx *c, double *xcorl, double *ycorl, double *uavg)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (c->nx > correlation_max_line() || c->ny > correlation_max_line())
+        return fail(c, DNSLBM_ERR_ARG, "correlation lines longer than %d cells", correlation_max_line());
+    CK(cudaSetDevice(c->deck.device));
+    const int zd = c->nz + 2;
+    const size_t cells = (size_t)c->nx * c->ny * zd;
+    int rc;
+    if ((rc = out_alloc(c, &c->out_vel, cells * 3)) || (rc = out_alloc(c, &c->out_den, cells))) return rc;
+    CK(cudaDeviceSynchronize());
+    if (c->out_pending) CK(cudaStreamWaitEvent(c->stream, c->out_ev[1], 0));
+    launch_io(c->deck.precision, 3, io_args(c), 0, c->nx, c->out_vel, c->out_den, c->stream);
+    CK(cudaGetLastError());
+    const cudaError_t e = correlations_of(c->out_vel, c->nx, c->ny, zd, c->stream, xcorl, ycorl, uavg);
+    if (e != cudaSuccess) return fail(c, DNSLBM_ERR_CUDA, "correlations: %s", cudaGetErrorString(e));
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_correlations_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *xcorl,
+                                       double *ycorl, double *uavg)
+{
+    dnslbm_ctx *c = nullptr;  // errors go to dnslbm_last_error(NULL)
+    if (!vel) return fail(c, DNSLBM_ERR_ARG, "null velocity field");
+    if (xdv < 1 || ydv < 1 || zdv < 1) return fail(c, DNSLBM_ERR_ARG, "grid %dx%dx%d too small", xdv, ydv, zdv);
+    if (xdv > correlation_max_line() || ydv > correlation_max_line())
+        return fail(c, DNSLBM_ERR_ARG, "correlation lines longer than %d cells", correlation_max_line());
+    const int zd = zdv + 2;
+    const size_t n = (size_t)xdv * ydv * zd * 3;
+    CK(cudaSetDevice(device));
+    double *dv = nullptr;
+    cudaError_t e = cudaMalloc(&dv, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(dv, vel, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = correlations_of(dv, xdv, ydv, zd, 0, xcorl, ycorl, uavg);
+    if (dv) cudaFree(dv);
+    if (e != cudaSuccess) return fail(c, DNSLBM_ERR_CUDA, "correlations of a velocity field: %s", cudaGetErrorString(e));
     return DNSLBM_OK;
 }
 

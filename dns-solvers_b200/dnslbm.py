@@ -80,6 +80,8 @@ def lib():
     L.dnslbm_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     L.dnslbm_quadrant.argtypes = [vp, dp, dp, dp]
     L.dnslbm_quadrant_vel.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp]
+    L.dnslbm_correlations.argtypes = [vp, dp, dp, dp]
+    L.dnslbm_correlations_vel.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.dnslbm_output_begin.argtypes = [vp, dp, dp, dp, dp]
     L.dnslbm_output_wait.argtypes = [vp]
     L.dnslbm_set_wait_limit.argtypes = [vp, ctypes.c_double]
@@ -197,6 +199,15 @@ class Channel:
         t, e, o = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         self._ck(self.L.dnslbm_step_timed(self.h, n, ctypes.byref(t), ctypes.byref(e), ctypes.byref(o)))
         return t.value, e.value, o.value
+
+    def correlations(self):
+        """Two-point correlations of the current state: (xcorl[zd][nx][3],
+        ycorl[zd][ny][3], uavg[zd]) as the reference's 2pt-correlations
+        program writes them."""
+        zd = self.shape[2] + 2
+        xc, yc, ua = np.zeros((zd, self.shape[0], 3)), np.zeros((zd, self.shape[1], 3)), np.zeros(zd)
+        self._ck(self.L.dnslbm_correlations(self.h, _dp(xc), _dp(yc), _dp(ua)))
+        return xc, yc, ua
 
     def quadrant(self):
         """Quadrant analysis of the current state: (quadrant[4][zd],
@@ -421,3 +432,17 @@ def quadrant_vel(vel, device=0):
     if rc:
         raise DnsLbmError(rc, L.dnslbm_last_error(None).decode())
     return q, dq, uw
+
+
+def correlations_vel(vel, device=0):
+    """Two-point correlations of a velocity field [xdv][ydv][zd][3] on the
+    GPU: (xcorl[zd][xdv][3], ycorl[zd][ydv][3], uavg[zd])."""
+    L = lib()
+    v = np.ascontiguousarray(vel, np.float64)
+    nx, ny, zd, three = v.shape
+    assert three == 3
+    xc, yc, ua = np.zeros((zd, nx, 3)), np.zeros((zd, ny, 3)), np.zeros(zd)
+    rc = L.dnslbm_correlations_vel(_dp(v), nx, ny, zd - 2, device, _dp(xc), _dp(yc), _dp(ua))
+    if rc:
+        raise DnsLbmError(rc, L.dnslbm_last_error(None).decode())
+    return xc, yc, ua

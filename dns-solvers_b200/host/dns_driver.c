@@ -23,6 +23,10 @@
  *               qUADrantA.c at every output event, on the GPU, from the live
  *               state: quadrant.000.TTTT and dquadrant.000.TTTT ([4][zd] then
  *               [zd] doubles)
+ *   CORREL 1    also the two-point correlations of 2pt-correlations/src
+ *               (mean_subtract.c, xcorrel.c, ycorrel.c) at every output
+ *               event, on the GPU: xcorl.TTTT ([zd][xdv][3]), ycorl.TTTT
+ *               ([zd][ydv][3]) and uavg.TTT ([zd]) doubles
  *   ASYNC 1|0   output without stopping the time loop (default 1): at an
  *               output step the library computes the outputs on the GPU and
  *               copies them to page-locked host buffers while the next steps
@@ -52,7 +56,7 @@
 typedef struct {
     double Rebs, ub, CFL, GX, OMEGA;
     int zdv, ydv, xdv, TSTR, TEND, ITER, RSLIP, PSLIP;
-    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS, ASYNC, QUADRANT;
+    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS, ASYNC, QUADRANT, CORREL;
     char TEXTURE[32], FORCE[8];
 } Deck;
 
@@ -90,7 +94,7 @@ static int deck_set(Deck *d, const char *k, const char *v)
 #define STR(N) if (!strcmp(k, #N)) { snprintf(d->N, sizeof d->N, "%s", v); return 0; }
     DBL(Rebs) DBL(ub) DBL(CFL) DBL(GX) DBL(OMEGA)
     INT(zdv) INT(ydv) INT(xdv) INT(TSTR) INT(TEND) INT(ITER) INT(RSLIP) INT(PSLIP)
-    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS) INT(ASYNC) INT(QUADRANT)
+    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS) INT(ASYNC) INT(QUADRANT) INT(CORREL)
     STR(TEXTURE) STR(FORCE)
 #undef DBL
 #undef INT
@@ -398,6 +402,24 @@ int main(int argc, char **argv)
                 if (qf) bad |= fclose(qf) != 0;
                 free(q);
                 if (bad) return die(c, DNSLBM_ERR_IO, qn);
+            }
+            if (D.CORREL) {
+                const size_t nxc = (size_t)zd * D.xdv * 3, nyc = (size_t)zd * D.ydv * 3;
+                double *r = malloc((nxc + nyc + (size_t)zd) * sizeof(double));
+                if (!r) return die(c, DNSLBM_ERR_IO, "host allocation");
+                if ((rc = dnslbm_correlations(c, r, r + nxc, r + nxc + nyc))) return die(c, rc, "dnslbm_correlations");
+                char cn[64];
+                const char *fmt[3] = {"xcorl.%.4d", "ycorl.%.4d", "uavg.%.3d"};
+                const size_t off[3] = {0, nxc, nxc + nyc}, len[3] = {nxc, nyc, (size_t)zd};
+                int bad = 0;
+                for (int f = 0; f < 3 && !bad; ++f) {
+                    snprintf(cn, sizeof cn, fmt[f], (int)sn->label);
+                    FILE *cf = fopen(cn, "wb");
+                    bad = !cf || fwrite(r + off[f], sizeof(double), len[f], cf) != len[f];
+                    if (cf) bad |= fclose(cf) != 0;
+                }
+                free(r);
+                if (bad) return die(c, DNSLBM_ERR_IO, cn);
             }
             if (D.ASYNC) {
                 /* the previous event's copies have landed (the steps since

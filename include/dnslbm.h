@@ -197,6 +197,29 @@ int dnslbm_quadrant(dnslbm_ctx *ctx, double *quadrant, double *dquadrant, double
 int dnslbm_quadrant_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *quadrant, double *dquadrant,
                         double *uw);
 
+/* Two-point velocity correlations of the current state, on the GPU
+ * (2pt-correlations/src/correlations.c: mean_subtract.c, xcorrel.c,
+ * ycorrel.c), from the cell velocities dnslbm_moments returns:
+ *   uavg[zd]          the subtracted mean of each plane: the plane mean of u
+ *                     over (x, y), made symmetric about the channel centre
+ *                     (u, v even, w odd); 0 on the wall planes, which keep
+ *                     their velocities (mean_subtract.c writes it to uavg.TTT);
+ *   xcorl[zd][xdv][3] per plane and component, the sum over (x, y) of
+ *                     u'(x, y) u'(x + d, y), d = 0 .. xdv-1 periodic
+ *                     (the program's xcorl.TTTT file);
+ *   ycorl[zd][ydv][3] the same along y (ycorl.TTTT).
+ * The sums are unnormalised, as the program writes them.  mean_subtract.c
+ * averages over the period of a stripe texture given at compile time; its
+ * shipped setting (no period) cannot run, and the plane mean here is its
+ * value for any period that divides the span.  Lines up to 2048 cells;
+ * temporary device memory of about 2.1 times the velocity field.  Any
+ * pointer may be NULL. */
+int dnslbm_correlations(dnslbm_ctx *ctx, double *xcorl, double *ycorl, double *uavg);
+/* The same for a velocity field read from a vel.NNNN file
+ * ([xdv][ydv][zdv+2][3] doubles), on CUDA device `device`. */
+int dnslbm_correlations_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *xcorl, double *ycorl,
+                            double *uavg);
+
 /* Timing support for benchmarks: advance nsteps like dnslbm_step and return
  * CUDA-event times on the context's stream: total, and the summed device
  * time of the two step kernels (even / odd parity launches). */

@@ -63,6 +63,8 @@ int MPI_Cart_rank(MPI_Comm c, const int *coords, int *rank);
 int MPI_Sendrecv(const void *sbuf, int scount, MPI_Datatype st, int dest, int stag,
                  void *rbuf, int rcount, MPI_Datatype rt, int src, int rtag,
                  MPI_Comm c, MPI_Status *status);
+int MPI_Sendrecv_replace(void *buf, int count, MPI_Datatype t, int dest, int stag, int src, int rtag, MPI_Comm c,
+                         MPI_Status *status);
 int MPI_Send_init(const void *buf, int count, MPI_Datatype t, int dest, int tag, MPI_Comm c, MPI_Request *req);
 int MPI_Recv_init(void *buf, int count, MPI_Datatype t, int src, int tag, MPI_Comm c, MPI_Request *req);
 int MPI_Startall(int n, MPI_Request *reqs);

@@ -120,6 +120,15 @@ int MPI_Sendrecv(const void *sbuf, int scount, MPI_Datatype st, int dest, int st
     return MPI_SUCCESS;
 }
 
+/* one rank sends to itself: the buffer holds what it sent */
+int MPI_Sendrecv_replace(void *buf, int count, MPI_Datatype t, int dest, int stag, int src, int rtag, MPI_Comm c,
+                         MPI_Status *status)
+{
+    (void)buf; (void)dest; (void)src; (void)c; (void)stag; (void)rtag;
+    if (status) status->count_bytes = (int)((long long)count * tsize(t));
+    return MPI_SUCCESS;
+}
+
 #define MAX_REQ 256
 typedef struct { void *buf; long long bytes; int tag; int is_send; int live; } stub_req;
 static stub_req reqs_tab[MAX_REQ];

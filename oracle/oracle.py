@@ -307,3 +307,75 @@ def quadrant_reference(vel, label=0, timeout=300):
         a = np.fromfile(os.path.join(td, f"quadrant.000.{label:04d}"))
         b = np.fromfile(os.path.join(td, f"dquadrant.000.{label:04d}"))
     return a[:4 * zd].reshape(4, zd), b[:4 * zd].reshape(4, zd), a[4 * zd:]
+
+
+CORR_BIN = os.path.join(HERE, "_ref", "corref")
+# the streamwise size the reference's 2pt-correlations program is compiled
+# for (its definitions.h xdv): xcorrel.c wraps its lags with it
+CORR_REF_NX = 512
+
+
+def mean_subtract(vel):
+    """2pt-correlations/src/mean_subtract.c restated (numpy, FP64): per plane
+    k = 1..zd-2 the means of u, v, w over (x, y) (mean_subtract.c:28-60 then
+    the average over the span, :197-213), made symmetric about the channel
+    centre -- u, v even, w odd (:178-196) -- and subtracted from the fluid
+    planes (:214-224); the wall planes keep their velocities.  The program
+    averages over the period (gplus + wplus) of a stripe texture first
+    (:80-177); its shipped setting, a period of 0, divides by zero, and for
+    any period that divides the span the span average of the phase averages
+    is the plane mean used here.  Returns (fluct, ua[zd][3]); ua[:, 0] is what
+    the program writes to uavg.TTT."""
+    vel = np.asarray(vel, np.float64)
+    nx, ny, zd, _ = vel.shape
+    m = np.zeros((zd, 3))
+    m[1:zd - 1] = vel[:, :, 1:zd - 1, :].sum(axis=(0, 1)) / (nx * ny)
+    ua = np.zeros((zd, 3))
+    k = np.arange(1, zd - 1)
+    kk = zd - 1 - k
+    ua[k, 0] = 0.5 * (m[k, 0] + m[kk, 0])
+    ua[k, 1] = 0.5 * (m[k, 1] + m[kk, 1])
+    ua[k, 2] = 0.5 * (m[k, 2] - m[kk, 2])
+    fl = vel.copy()
+    fl[:, :, 1:zd - 1, :] -= ua[None, None, 1:zd - 1, :]
+    return fl, ua
+
+
+def correlations(vel):
+    """The program's correlations of one velocity field (correlations.c:124-
+    128): mean_subtract, then ycorrel.c and xcorrel.c restated:
+    xcorl[k][d][c] = sum over (x, y) of u'_c(x, y, k) u'_c(x+d, y, k) and
+    ycorl[k][d][c] = sum over (x, y) of u'_c(x, y, k) u'_c(x, y+d, k), lags
+    periodic, every plane k = 0..zd-1, unnormalised.  Returns (xcorl
+    [zd][nx][3], ycorl [zd][ny][3], uavg [zd])."""
+    fl, ua = mean_subtract(vel)
+    nx, ny, zd, _ = fl.shape
+    xc = np.zeros((zd, nx, 3))
+    yc = np.zeros((zd, ny, 3))
+    for d in range(nx):
+        xc[:, d, :] = (fl * np.roll(fl, -d, axis=0)).sum(axis=(0, 1))
+    for d in range(ny):
+        yc[:, d, :] = (fl * np.roll(fl, -d, axis=1)).sum(axis=(0, 1))
+    return xc, yc, ua[:, 0].copy()
+
+
+def have_correlation_reference() -> bool:
+    return os.path.exists(CORR_BIN)
+
+
+def correlations_reference(fluct, label=0, timeout=600):
+    """The reference's own ycorrel and xcorrel (oracle/_ref/corref) on a
+    fluctuation field [nx][ny][zd][3] with nx = CORR_REF_NX; returns (xcorl
+    [zd][nx][3], ycorl [zd][ny][3]) as the program writes them."""
+    if not have_correlation_reference():
+        raise FileNotFoundError(CORR_BIN)
+    nx, ny, zd, _ = fluct.shape
+    if nx != CORR_REF_NX:
+        raise ValueError(f"the reference's xcorrel is compiled for nx = {CORR_REF_NX}")
+    with tempfile.TemporaryDirectory() as td:
+        np.ascontiguousarray(fluct, np.float64).tofile(os.path.join(td, "fluct.bin"))
+        subprocess.run([CORR_BIN, str(nx), str(ny), str(zd - 2), "fluct.bin", str(label)], cwd=td, check=True,
+                       timeout=timeout, stdout=subprocess.DEVNULL)
+        xc = np.fromfile(os.path.join(td, f"xcorl.{label:04d}")).reshape(zd, nx, 3)
+        yc = np.fromfile(os.path.join(td, f"ycorl.{label:04d}")).reshape(zd, ny, 3)
+    return xc, yc

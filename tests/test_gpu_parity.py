@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 # step goldens (the quadrant-analysis fixtures are tests/test_quadrant.py's)
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("quadrant_"))
+                if not os.path.basename(p).startswith(("quadrant_", "correl_")))
 
 
 def gpu_run(s0, flags, omega, steps, gx=0.0, ubulk=0.0, const_g=True, precision=64, chunks=None):

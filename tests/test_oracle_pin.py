@@ -16,7 +16,7 @@ import inputs
 
 # step goldens (the quadrant-analysis fixtures are tests/test_quadrant.py's)
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("quadrant_"))
+                if not os.path.basename(p).startswith(("quadrant_", "correl_")))
 LOG_COLS = ("energy", "flowrate", "massrate", "stup", "stdown", "stress", "pgrad")
 
 
