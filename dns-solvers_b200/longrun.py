@@ -174,10 +174,23 @@ def compare(ref, o):
             e[f"{name}_max_rel"] = rel
             e[f"{name}_sigma_rel"] = sig
             e[f"{name}_max_z"] = z
+    # the folded mean-u profile over the half channel: RMS difference, RMS
+    # sampling error, and the mean of (difference / sigma)^2 (about 1 when
+    # the difference is sampling noise)
+    h = len(ref["mean_u_fold"]) // 2
+    scale = max(np.max(np.abs(ref["mean_u"])), 1e-300)
+    d = (o["mean_u_fold"] - ref["mean_u_fold"])[:h]
+    sig = np.sqrt(ref["mean_u_fold_se"] ** 2 + o["mean_u_fold_se"] ** 2)[:h]
+    e["mean_u_fold_rms_rel"] = float(np.sqrt(np.mean(d ** 2)) / scale)
+    e["mean_u_fold_rms_sigma_rel"] = float(np.sqrt(np.mean(sig ** 2)) / scale)
+    e["mean_u_fold_mean_rel"] = float(np.mean(d) / scale)
+    if np.all(sig > 0):
+        e["mean_u_fold_chi2_per_plane"] = float(np.mean((d / sig) ** 2))
     for k in ("re_tau", "cf", "u_bulk", "tau_w"):
         e[f"{k}_rel"] = abs(o[k] - ref[k]) / abs(ref[k])
         sig = math.sqrt(ref[k + "_se"] ** 2 + o[k + "_se"] ** 2)
         e[f"{k}_sigma_rel"] = sig / abs(ref[k])
+        e[f"{k}_z"] = abs(o[k] - ref[k]) / sig if sig > 0 else float("inf")
     if "slip_u_first_plane" in ref:
         e["slip_u_rel"] = abs(o["slip_u_first_plane"] - ref["slip_u_first_plane"]) / abs(ref["slip_u_first_plane"])
     return e
@@ -197,18 +210,21 @@ def main():
     ap.add_argument("--out", default=None)
     ap.add_argument("--save", default=None, help="write the runs' block averages (.npz) for a later --ref")
     ap.add_argument("--ref", default=None, help="runs saved by --save: a listed run found there is not run again")
+    ap.add_argument("--runs-command", default=None, help="the command that made the runs of --ref (recorded)")
     a = ap.parse_args()
     saved = load_runs(a.ref) if a.ref else {}
     wl = inputs.workload(a.workload)
     flags = inputs.make_flags(wl)
-    s0 = inputs.make_state(wl, seed=a.seed)
-    if inputs.needs_general(wl):
-        s0 = inputs.rest_solids(s0, flags)
+    s0 = None  # made when a run is needed (the runs of --ref are not run again)
     runs = []
     for p in a.precisions.split(","):
         if p in saved:
             runs.append(saved[p])
             continue
+        if s0 is None:
+            s0 = inputs.make_state(wl, seed=a.seed)
+            if inputs.needs_general(wl):
+                s0 = inputs.rest_solids(s0, flags)
         init = s0
         if p.startswith("64p"):
             amp = float(p[3:]) if len(p) > 3 else a.control_amp
@@ -224,8 +240,10 @@ def main():
         runs.append(r)
     ref = runs[0]
     summary = {"workload": wl.name, "grid": f"{wl.nx}x{wl.nz + 2}x{wl.ny}", "texture": wl.texture,
-               "command": " ".join(sys.argv), "spinup": a.spinup, "steps": a.steps, "sample_every": a.sample,
+               "command": "python " + " ".join(sys.argv), "spinup": a.spinup, "steps": a.steps, "sample_every": a.sample,
                "blocks": a.blocks, "seed": a.seed, "control_amp": a.control_amp, "runs": []}
+    if a.runs_command:
+        summary["runs_command"] = a.runs_command
     if inputs.needs_general(wl):
         summary["note"] = ("walls with riblets: the reference's wall-stress formula (a one-sided difference of "
                            "plane means at a flat wall) does not measure the riblet drag; compare u_bulk at "
