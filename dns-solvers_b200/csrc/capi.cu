@@ -1709,9 +1709,10 @@ static int persist_configure(dnslbm_batch *b)
 }
 
 // One launch shape for all channels: per channel the most rows per stage
-// group (1, 2, 4 or 8) whose `stages` groups fit `budget` bytes; the block
-// takes the largest of these.  Returns 0 and selects the shape when it runs
-// on the device.
+// group (up to 16) whose `stages` groups fit `budget` bytes, so channels of
+// short rows move about as many bytes per stage as those of long rows; the
+// block takes the largest of these stages.  Returns 0 and selects the shape
+// when it runs on the device.
 static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consumers)
 {
     consumers = std::max(32, std::min(352, consumers / 32 * 32));
@@ -1723,7 +1724,7 @@ static int batch_configure(dnslbm_batch *b, size_t budget, int stages, int consu
         auto need = [&](int k) { return (size_t)stages * Q * row_bytes * k + 16 * (size_t)stages; };
         if (need(1) > budget) return -1;
         int k = 1;
-        while (k < 8 && 2 * k <= c->ny && need(2 * k) <= budget) k *= 2;
+        while (k < 16 && k + 1 <= c->ny && need(k + 1) <= budget) ++k;
         ks[i] = k;
         smem = std::max(smem, need(k));
     }
