@@ -30,6 +30,9 @@ size_t correlation_scratch(int nx, int ny, int zd, int per_chunk);
 int correlation_max_line();
 cudaError_t launch_correlations(const double *vel, int nx, int ny, int zd, int per_chunk, double *scratch,
                                 double *xcorl, double *ycorl, double *ua, cudaStream_t s);
+size_t spectra_scratch(int nx, int ny, int zd, int jb);
+cudaError_t launch_spectra(const double *vel, int nx, int ny, int zd, int jb, double *scratch, double *ex, double *ey,
+                           cudaStream_t s);
 int persist_prepare_f64(size_t smem);
 int persist_occupancy_f64(int threads, size_t smem, bool any_q);
 cudaError_t launch_persist_f64(const PersistArgs &a, int grid, int threads, size_t smem, bool any_q, cudaStream_t s);
@@ -1291,6 +1294,75 @@ extern "C" int dnslbm_correlations_vel(const double *vel, int xdv, int ydv, int 
     if (e == cudaSuccess) e = correlations_of(dv, xdv, ydv, zd, 0, xcorl, ycorl, uavg);
     if (dv) cudaFree(dv);
     if (e != cudaSuccess) return fail(c, DNSLBM_ERR_CUDA, "correlations of a velocity field: %s", cudaGetErrorString(e));
+    return DNSLBM_OK;
+}
+
+// One-dimensional energy spectra (e-spectra/src/1d-spectra.c) of a velocity
+// field in device memory; results in the program's file layouts: ex
+// [3][nx][zd] (Euux, Evvx, Ewwx), ey [3][ny/2+1][zd] (Euuy, Evvy, Ewwy).
+static cudaError_t spectra_of(const double *dvel, int nx, int ny, int zd, cudaStream_t s, double *ex, double *ey)
+{
+    const int nj = ny / 2 + 1, nzf = zd - 2;
+    const int jb = std::max(1, std::min(8, (int)((180 * 1024) / (16 * (size_t)nx)) - 1));
+    double *scratch = nullptr, *res = nullptr;
+    const size_t nres = (size_t)nzf * 3 * (nx + nj);
+    cudaError_t e = cudaMalloc(&scratch, spectra_scratch(nx, ny, zd, jb) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&res, nres * sizeof(double));
+    if (e == cudaSuccess) e = launch_spectra(dvel, nx, ny, zd, jb, scratch, res, res + (size_t)nzf * 3 * nx, s);
+    std::vector<double> h(nres);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), res, nres * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (scratch) cudaFree(scratch);
+    if (res) cudaFree(res);
+    if (e != cudaSuccess) return e;
+    const double *hx = h.data(), *hy = h.data() + (size_t)nzf * 3 * nx;
+    for (int c = 0; c < 3; ++c) {
+        if (ex)
+            for (int i = 0; i < nx; ++i)
+                for (int k = 0; k < zd; ++k)
+                    ex[((size_t)c * nx + i) * zd + k] =
+                        (k == 0 || k == zd - 1) ? 0.0 : hx[((size_t)(k - 1) * 3 + c) * nx + i];
+        if (ey)
+            for (int j = 0; j < nj; ++j)
+                for (int k = 0; k < zd; ++k)
+                    ey[((size_t)c * nj + j) * zd + k] =
+                        (k == 0 || k == zd - 1) ? 0.0 : hy[((size_t)(k - 1) * 3 + c) * nj + j];
+    }
+    return cudaSuccess;
+}
+
+extern "C" int dnslbm_spectra(dnslbm_ctx *c, double *ex, double *ey)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    CK(cudaSetDevice(c->deck.device));
+    const int zd = c->nz + 2;
+    const size_t cells = (size_t)c->nx * c->ny * zd;
+    int rc;
+    if ((rc = out_alloc(c, &c->out_vel, cells * 3)) || (rc = out_alloc(c, &c->out_den, cells))) return rc;
+    CK(cudaDeviceSynchronize());
+    if (c->out_pending) CK(cudaStreamWaitEvent(c->stream, c->out_ev[1], 0));
+    launch_io(c->deck.precision, 3, io_args(c), 0, c->nx, c->out_vel, c->out_den, c->stream);
+    CK(cudaGetLastError());
+    const cudaError_t e = spectra_of(c->out_vel, c->nx, c->ny, zd, c->stream, ex, ey);
+    if (e != cudaSuccess) return fail(c, DNSLBM_ERR_CUDA, "spectra: %s", cudaGetErrorString(e));
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_spectra_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *ex, double *ey)
+{
+    dnslbm_ctx *c = nullptr;  // errors go to dnslbm_last_error(NULL)
+    if (!vel) return fail(c, DNSLBM_ERR_ARG, "null velocity field");
+    if (xdv < 1 || ydv < 1 || zdv < 1) return fail(c, DNSLBM_ERR_ARG, "grid %dx%dx%d too small", xdv, ydv, zdv);
+    const int zd = zdv + 2;
+    const size_t n = (size_t)xdv * ydv * zd * 3;
+    CK(cudaSetDevice(device));
+    double *dv = nullptr;
+    cudaError_t e = cudaMalloc(&dv, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(dv, vel, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = spectra_of(dv, xdv, ydv, zd, 0, ex, ey);
+    if (dv) cudaFree(dv);
+    if (e != cudaSuccess) return fail(c, DNSLBM_ERR_CUDA, "spectra of a velocity field: %s", cudaGetErrorString(e));
     return DNSLBM_OK;
 }
 

@@ -212,3 +212,166 @@ cudaError_t launch_correlations(const double *vel, int nx, int ny, int zd, int p
 }
 
 }  // namespace dnslbm
+
+namespace dnslbm {
+
+// ------------------------------------------------------------------ spectra
+// One-dimensional energy spectra of the reference's e-spectra program
+// (e-spectra/src/1d-spectra.c), one velocity field.  Per fluid plane k and
+// component c: the 2-D real-to-complex DFT over (x, y) (FFTW's r2c_2d,
+// C[i][j] = sum_{x,y} u(x, y) e^{-2 pi i (i x / nx + j y / ny)}, i < nx,
+// j <= ny/2), scaled by 2 / (2 nx ny) (:131-143), the (0, 0) mode set to 0
+// (:146-151), then p = 0.5 fac_j |C|^2 with fac_0 = 1, fac_j = 2 otherwise
+// (:156-172), summed over j into E_x[i][k] and over i into E_y[j][k]; the
+// wall planes are 0.  The DFT is evaluated directly in FP64 (two passes: the
+// half spectrum along y for every x line, then the full transform along x of
+// every kept y mode), with exact twiddle factors sincospi(2 m / n), m = n*index
+// mod n; the sums are FP64 in a fixed order.  Output files Euux/Evvx/Ewwx
+// ([nx][zd] each) and Euuy/Evvy/Ewwy ([ny/2+1][zd] each).
+
+constexpr int kSpecThreads = 256;
+
+// twiddles: tw[m] = (cos(2 pi m / n), -sin(2 pi m / n)), m < n
+__global__ void spec_twiddle_kernel(int n, double2 *tw)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    double s, c;
+    sincospi(2.0 * (double)m / (double)n, &s, &c);
+    tw[m] = make_double2(c, -s);
+}
+
+// pass 1: V[k][c][j][x] = sum_y u(x, y, k, c) tw_y[(j y) mod ny], j < nj
+// grid (ceil(nx / lines), zd - 2, 3); one x line per warp-sized group
+__global__ void __launch_bounds__(kSpecThreads) spec_y_kernel(const double *__restrict__ vel,
+                                                              const double2 *__restrict__ twy, int nx, int ny,
+                                                              int zd, int nj, int lines, double2 *V)
+{
+    extern __shared__ double sm[];  // twiddles (2 ny), then `lines` lines of ny
+    double2 *tw = reinterpret_cast<double2 *>(sm);
+    double *ln = sm + 2 * ny;
+    const int x0 = blockIdx.x * lines, k = blockIdx.y + 1, c = blockIdx.z;
+    const int nl = min(lines, nx - x0);
+    for (int m = threadIdx.x; m < ny; m += blockDim.x) tw[m] = twy[m];
+    for (int e = threadIdx.x; e < nl * ny; e += blockDim.x) {
+        const int l = e / ny, y = e - l * ny;
+        ln[e] = vel[(((size_t)(x0 + l) * ny + y) * zd + k) * 3 + c];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nl * nj; e += blockDim.x) {
+        const int l = e / nj, j = e - l * nj;
+        const double *u = ln + (size_t)l * ny;
+        double re = 0.0, im = 0.0;
+        int m = 0;
+        for (int y = 0; y < ny; ++y) {
+            const double2 w = tw[m];
+            re = fma(u[y], w.x, re);
+            im = fma(u[y], w.y, im);
+            m += j;
+            if (m >= ny) m -= ny;
+        }
+        V[(((size_t)blockIdx.y * 3 + c) * nj + j) * nx + x0 + l] = make_double2(re, im);
+    }
+}
+
+// pass 2: C[i][j] = sum_x V[j][x] tw_x[(i x) mod nx] for the block's `jb` modes
+// j; p = 0.5 fac_j |s C|^2 (C[0][0] = 0); ey[k][c][j] = sum_i p, and the
+// block's partial sum over its j of p per i in part[chunk][k][c][i]
+__global__ void __launch_bounds__(kSpecThreads) spec_x_kernel(const double2 *__restrict__ V,
+                                                              const double2 *__restrict__ twx, int nx, int nj,
+                                                              int zd, int jb, double scale, double *ey,
+                                                              double *part)
+{
+    extern __shared__ double sm[];
+    double2 *tw = reinterpret_cast<double2 *>(sm);  // nx twiddles, then jb columns of nx
+    double2 *col = tw + nx;
+    __shared__ double red[32];
+    const int j0 = blockIdx.x * jb, kk = blockIdx.y, c = blockIdx.z;
+    const int nb = min(jb, nj - j0);
+    for (int m = threadIdx.x; m < nx; m += blockDim.x) tw[m] = twx[m];
+    const double2 *src = V + (((size_t)kk * 3 + c) * nj + j0) * nx;
+    for (int e = threadIdx.x; e < nb * nx; e += blockDim.x) col[e] = src[e];
+    __syncthreads();
+    double *pout = part + (((size_t)blockIdx.x * (zd - 2) + kk) * 3 + c) * nx;
+    for (int i0 = 0; i0 < nx; i0 += blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        double px = 0.0;
+        for (int b = 0; b < nb; ++b) {
+            const int j = j0 + b;
+            double p = 0.0;
+            if (i < nx) {
+                const double2 *v = col + (size_t)b * nx;
+                double re = 0.0, im = 0.0;
+                int m = 0;
+                for (int x = 0; x < nx; ++x) {
+                    const double2 w = tw[m], a = v[x];
+                    re = fma(a.x, w.x, re);
+                    re = fma(-a.y, w.y, re);
+                    im = fma(a.x, w.y, im);
+                    im = fma(a.y, w.x, im);
+                    m += i;
+                    if (m >= nx) m -= nx;
+                }
+                re *= scale;
+                im *= scale;
+                if (i == 0 && j == 0) re = im = 0.0;
+                p = (j == 0 ? 0.5 : 1.0) * (re * re + im * im);
+                px += p;
+            }
+            // the block's sum over i for mode j, in a fixed order
+            double s[1] = {p};
+            block_sum<1>(s, red);
+            if (threadIdx.x == 0) {
+                double *dst = ey + (((size_t)kk * 3 + c) * nj + j);
+                *dst = (i0 == 0 ? 0.0 : *dst) + s[0];
+            }
+            __syncthreads();
+        }
+        if (i < nx) pout[i] = px;
+    }
+}
+
+// E_x[k][c][i] = sum over the j chunks of part, in chunk order
+__global__ void spec_reduce_kernel(const double *__restrict__ part, int nchunks, int nx, int nzf, double *ex)
+{
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t n = (size_t)nzf * 3 * nx;
+    if (idx >= n) return;
+    double s = 0.0;
+    for (int ch = 0; ch < nchunks; ++ch) s += part[(size_t)ch * n + idx];
+    ex[idx] = s;
+}
+
+// Scratch of launch_spectra, in doubles.
+size_t spectra_scratch(int nx, int ny, int zd, int jb)
+{
+    const int nj = ny / 2 + 1, chunks = (nj + jb - 1) / jb;
+    return 2 * (size_t)(nx + ny) + 2 * (size_t)(zd - 2) * 3 * nj * nx + (size_t)chunks * (zd - 2) * 3 * nx;
+}
+
+// ex [zd-2][3][nx], ey [zd-2][3][ny/2+1] in device memory (fluid planes)
+cudaError_t launch_spectra(const double *vel, int nx, int ny, int zd, int jb, double *scratch, double *ex, double *ey,
+                           cudaStream_t s)
+{
+    const int nj = ny / 2 + 1, nzf = zd - 2, chunks = (nj + jb - 1) / jb;
+    double2 *twx = reinterpret_cast<double2 *>(scratch), *twy = twx + nx;
+    double2 *V = twy + ny;
+    double *part = reinterpret_cast<double *>(V + (size_t)nzf * 3 * nj * nx);
+    const size_t sm1_lines = 8;
+    const size_t sm1 = (2 * (size_t)ny + sm1_lines * ny) * sizeof(double);
+    const size_t sm2 = ((size_t)nx + (size_t)jb * nx) * sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(spec_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(spec_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+    if (e != cudaSuccess) return e;
+    spec_twiddle_kernel<<<(nx + 255) / 256, 256, 0, s>>>(nx, twx);
+    spec_twiddle_kernel<<<(ny + 255) / 256, 256, 0, s>>>(ny, twy);
+    spec_y_kernel<<<dim3((nx + (int)sm1_lines - 1) / (int)sm1_lines, nzf, 3), kSpecThreads, sm1, s>>>(
+        vel, twy, nx, ny, zd, nj, (int)sm1_lines, V);
+    spec_x_kernel<<<dim3(chunks, nzf, 3), kSpecThreads, sm2, s>>>(V, twx, nx, nj, zd, jb,
+                                                                    2.0 * (1.0 / (2.0 * nx * ny)), ey, part);
+    spec_reduce_kernel<<<(unsigned)(((size_t)nzf * 3 * nx + 255) / 256), 256, 0, s>>>(part, chunks, nx, nzf, ex);
+    return cudaGetLastError();
+}
+
+}  // namespace dnslbm

@@ -81,6 +81,8 @@ def lib():
     L.dnslbm_quadrant.argtypes = [vp, dp, dp, dp]
     L.dnslbm_quadrant_vel.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.dnslbm_correlations.argtypes = [vp, dp, dp, dp]
+    L.dnslbm_spectra.argtypes = [vp, dp, dp]
+    L.dnslbm_spectra_vel.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
     L.dnslbm_correlations_vel.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.dnslbm_output_begin.argtypes = [vp, dp, dp, dp, dp]
     L.dnslbm_output_wait.argtypes = [vp]
@@ -208,6 +210,15 @@ class Channel:
         xc, yc, ua = np.zeros((zd, self.shape[0], 3)), np.zeros((zd, self.shape[1], 3)), np.zeros(zd)
         self._ck(self.L.dnslbm_correlations(self.h, _dp(xc), _dp(yc), _dp(ua)))
         return xc, yc, ua
+
+    def spectra(self):
+        """One-dimensional energy spectra of the current state: (ex[3][nx][zd],
+        ey[3][ny//2+1][zd]) as the reference's e-spectra program writes
+        Euux/Evvx/Ewwx and Euuy/Evvy/Ewwy."""
+        nx, ny, nz = self.shape
+        ex, ey = np.zeros((3, nx, nz + 2)), np.zeros((3, ny // 2 + 1, nz + 2))
+        self._ck(self.L.dnslbm_spectra(self.h, _dp(ex), _dp(ey)))
+        return ex, ey
 
     def quadrant(self):
         """Quadrant analysis of the current state: (quadrant[4][zd],
@@ -446,3 +457,17 @@ def correlations_vel(vel, device=0):
     if rc:
         raise DnsLbmError(rc, L.dnslbm_last_error(None).decode())
     return xc, yc, ua
+
+
+def spectra_vel(vel, device=0):
+    """One-dimensional energy spectra of a velocity field [xdv][ydv][zd][3]
+    on the GPU: (ex[3][xdv][zd], ey[3][ydv//2+1][zd])."""
+    L = lib()
+    v = np.ascontiguousarray(vel, np.float64)
+    nx, ny, zd, three = v.shape
+    assert three == 3
+    ex, ey = np.zeros((3, nx, zd)), np.zeros((3, ny // 2 + 1, zd))
+    rc = L.dnslbm_spectra_vel(_dp(v), nx, ny, zd - 2, device, _dp(ex), _dp(ey))
+    if rc:
+        raise DnsLbmError(rc, L.dnslbm_last_error(None).decode())
+    return ex, ey

@@ -27,6 +27,10 @@
  *               (mean_subtract.c, xcorrel.c, ycorrel.c) at every output
  *               event, on the GPU: xcorl.TTTT ([zd][xdv][3]), ycorl.TTTT
  *               ([zd][ydv][3]) and uavg.TTT ([zd]) doubles
+ *   SPECTRA 1   also the one-dimensional energy spectra of e-spectra/src/
+ *               1d-spectra.c at every output event, on the GPU: Euux.TTTT,
+ *               Evvx.TTTT, Ewwx.TTTT ([xdv][zd]) and Euuy, Evvy, Ewwy
+ *               ([ydv/2+1][zd]) doubles
  *   ASYNC 1|0   output without stopping the time loop (default 1): at an
  *               output step the library computes the outputs on the GPU and
  *               copies them to page-locked host buffers while the next steps
@@ -56,7 +60,7 @@
 typedef struct {
     double Rebs, ub, CFL, GX, OMEGA;
     int zdv, ydv, xdv, TSTR, TEND, ITER, RSLIP, PSLIP;
-    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS, ASYNC, QUADRANT, CORREL;
+    int PRECISION, DEVICE, GAP, WIDTH, PGX, PWX, PGY, PWY, RIBH, RIBS, ASYNC, QUADRANT, CORREL, SPECTRA;
     char TEXTURE[32], FORCE[8];
 } Deck;
 
@@ -94,7 +98,7 @@ static int deck_set(Deck *d, const char *k, const char *v)
 #define STR(N) if (!strcmp(k, #N)) { snprintf(d->N, sizeof d->N, "%s", v); return 0; }
     DBL(Rebs) DBL(ub) DBL(CFL) DBL(GX) DBL(OMEGA)
     INT(zdv) INT(ydv) INT(xdv) INT(TSTR) INT(TEND) INT(ITER) INT(RSLIP) INT(PSLIP)
-    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS) INT(ASYNC) INT(QUADRANT) INT(CORREL)
+    INT(PRECISION) INT(DEVICE) INT(GAP) INT(WIDTH) INT(PGX) INT(PWX) INT(PGY) INT(PWY) INT(RIBH) INT(RIBS) INT(ASYNC) INT(QUADRANT) INT(CORREL) INT(SPECTRA)
     STR(TEXTURE) STR(FORCE)
 #undef DBL
 #undef INT
@@ -420,6 +424,25 @@ int main(int argc, char **argv)
                 }
                 free(r);
                 if (bad) return die(c, DNSLBM_ERR_IO, cn);
+            }
+            if (D.SPECTRA) {
+                const size_t nex = (size_t)D.xdv * zd, ney = (size_t)(D.ydv / 2 + 1) * zd;
+                double *r = malloc(3 * (nex + ney) * sizeof(double));
+                if (!r) return die(c, DNSLBM_ERR_IO, "host allocation");
+                if ((rc = dnslbm_spectra(c, r, r + 3 * nex))) return die(c, rc, "dnslbm_spectra");
+                static const char *name[6] = {"Euux", "Evvx", "Ewwx", "Euuy", "Evvy", "Ewwy"};
+                char sn_[64];
+                int bad = 0;
+                for (int f = 0; f < 6 && !bad; ++f) {
+                    const double *src = f < 3 ? r + f * nex : r + 3 * nex + (f - 3) * ney;
+                    const size_t len = f < 3 ? nex : ney;
+                    snprintf(sn_, sizeof sn_, "%s.%.4d", name[f], (int)sn->label);
+                    FILE *sf = fopen(sn_, "wb");
+                    bad = !sf || fwrite(src, sizeof(double), len, sf) != len;
+                    if (sf) bad |= fclose(sf) != 0;
+                }
+                free(r);
+                if (bad) return die(c, DNSLBM_ERR_IO, sn_);
             }
             if (D.ASYNC) {
                 /* the previous event's copies have landed (the steps since

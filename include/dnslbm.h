@@ -220,6 +220,20 @@ int dnslbm_correlations(dnslbm_ctx *ctx, double *xcorl, double *ycorl, double *u
 int dnslbm_correlations_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *xcorl, double *ycorl,
                             double *uavg);
 
+/* One-dimensional energy spectra of the current state, on the GPU
+ * (e-spectra/src/1d-spectra.c): per fluid plane, the 2-D DFT of u, v, w
+ * over (x, y) scaled by 1/(xdv ydv) with the mean mode removed, and
+ * 0.5 |C|^2 summed over the half spectrum in y (modes j > 0 twice) into
+ *   ex[3][xdv][zd]       Euux, Evvx, Ewwx (per streamwise mode i),
+ *   ey[3][ydv/2+1][zd]   Euuy, Evvy, Ewwy (per spanwise mode j),
+ * the program's file layouts ([mode][zd] per component, wall planes 0).  The
+ * transforms are evaluated directly in FP64 (the program calls FFTW), to
+ * rounding of the DFT.  Either pointer may be NULL. */
+int dnslbm_spectra(dnslbm_ctx *ctx, double *ex, double *ey);
+/* The same for a velocity field read from a vel.NNNN file
+ * ([xdv][ydv][zdv+2][3] doubles), on CUDA device `device`. */
+int dnslbm_spectra_vel(const double *vel, int xdv, int ydv, int zdv, int device, double *ex, double *ey);
+
 /* Timing support for benchmarks: advance nsteps like dnslbm_step and return
  * CUDA-event times on the context's stream: total, and the summed device
  * time of the two step kernels (even / odd parity launches). */

@@ -379,3 +379,32 @@ def correlations_reference(fluct, label=0, timeout=600):
         xc = np.fromfile(os.path.join(td, f"xcorl.{label:04d}")).reshape(zd, nx, 3)
         yc = np.fromfile(os.path.join(td, f"ycorl.{label:04d}")).reshape(zd, ny, 3)
     return xc, yc
+
+
+def spectra(vel):
+    """e-spectra/src/1d-spectra.c restated (numpy, FP64).  The program calls
+    FFTW 3 (fftw_mpi_plan_dft_r2c_2d, version not pinned by the reference,
+    not vendored); r2c_2d computes the unnormalised 2-D DFT C[i][j] =
+    sum_{x,y} u(x,y) exp(-2 pi i (i x / nx + j y / ny)) for i < nx, j <=
+    ny/2, which numpy's rfft2 computes too.  Per fluid plane k (:116-128):
+    the DFT of u, v, w; scaled by 2 / (2 nx ny) (:131-143); the (0, 0) mode
+    set to 0 (:146-151); p = fac_j 0.5 |C|^2, fac_0 = 1 and fac_j = 2 for
+    j > 0 (:156-172), summed over j into Euux[i][k] and over i into
+    Euuy[j][k].  Returns (ex[3][nx][zd], ey[3][ny//2+1][zd]); wall planes
+    0."""
+    vel = np.asarray(vel, np.float64)
+    nx, ny, zd, _ = vel.shape
+    nj = ny // 2 + 1
+    ex = np.zeros((3, nx, zd))
+    ey = np.zeros((3, nj, zd))
+    fac = np.full(nj, 2.0)
+    fac[0] = 1.0
+    scale = 2.0 * (1.0 / (2.0 * nx * ny))
+    for k in range(1, zd - 1):
+        for c in range(3):
+            C = np.fft.rfft2(vel[:, :, k, c]) * scale
+            C[0, 0] = 0.0
+            p = 0.5 * fac[None, :] * (C.real ** 2 + C.imag ** 2)
+            ex[c, :, k] = p.sum(axis=1)
+            ey[c, :, k] = p.sum(axis=0)
+    return ex, ey
