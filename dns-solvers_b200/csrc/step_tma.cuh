@@ -211,18 +211,6 @@ __device__ __forceinline__ void copy_group(const StepArgs &p, const TmaArgs &t, 
 // writes x0-1 .. x1-2 and the store covers [x0, x0+E).  The elements outside
 // (at most two per segment and direction) are written by their cells
 // directly (tma_group, SEG).
-// With seg_halo (FP64 rows of even length), a shifted direction also loads
-// its two halo pairs, 16 bytes each: elements x0-2, x0-1 (periodic: nx-2,
-// nx-1 for x0 = 0) to indices 0, 1 and x1, x1+1 (0, 1 for x1 = nx) to L+2,
-// L+3, so every cell of the segment reads its e_x-shifted element from shared
-// memory (an edge cell's element is its own address, which no other cell of
-// the step writes).
-template <typename T>
-__host__ __device__ __forceinline__ bool seg_halo(int nx)
-{
-    return sizeof(T) == 8 && (nx & 1) == 0;
-}
-
 template <typename T>
 __device__ __forceinline__ void copy_segment(const StepArgs &p, const GroupRows &g, int x0, int x1, int shift,
                                              unsigned char *sdir, bool to_smem, uint64_t *bar)
@@ -233,11 +221,6 @@ __device__ __forceinline__ void copy_segment(const StepArgs &p, const GroupRows 
     T *row = static_cast<T *>(p.pop[g.slot]) + (size_t)(g.zz * ny + y) * p.pitch;
     if (to_smem) {
         bulk_g2s(sdir + 2 * sizeof(T), row + x0, (uint32_t)(Lp * sizeof(T)), bar);
-        if (shift != 0 && seg_halo<T>(p.nx)) {
-            bulk_g2s(sdir, row + (x0 >= 2 ? x0 - 2 : p.nx - 2), (uint32_t)(2 * sizeof(T)), bar);
-            bulk_g2s(sdir + (size_t)(L + 2) * sizeof(T), row + (x1 + 2 <= p.nx ? x1 : 0), (uint32_t)(2 * sizeof(T)),
-                     bar);
-        }
         return;
     }
     const int E = (L - 1) & ~1;
@@ -265,7 +248,6 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
     const int nx = p.nx, pitch = p.pitch;
     if (!SEG) x0 = 0, x1 = nx;
     const int sxoff = SEG ? 2 - x0 : 0;  // shared-memory index of element x: x + sxoff
-    [[maybe_unused]] const bool halo = SEG && seg_halo<T>(nx);
     // low precision: a row's few cells per thread are summed in FP32, then
     // added to the FP64 accumulators when the thread moves to another row
     float racc[NP];
@@ -304,12 +286,8 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
                 v = ld_glb<T>(static_cast<const T *>(p.pop[slot]) + idx);
             } else {
                 const int xs = (ODD && !wdir) ? (lat_ex(A) > 0 ? xp : (lat_ex(A) < 0 ? xm : x)) : x;
-                if (SEG && edge && !wdir && lat_ex(A) != 0) {
-                    if (halo) v = ld_raw<T>(sbj + A * dstride + x + lat_ex(A));  // the halo pair, unwrapped index
-                    else v = ld_glb<T>(shifted_ptr(A, xs));
-                } else {
-                    v = ld_raw<T>(sbj + A * dstride + xs);
-                }
+                if (SEG && edge && !wdir && lat_ex(A) != 0) v = ld_glb<T>(shifted_ptr(A, xs));
+                else v = ld_raw<T>(sbj + A * dstride + xs);
             }
             f[ODD ? lat_opp(A) : A] = v;
         }
@@ -639,8 +617,6 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             GroupRows g{};
             if (lane < Q) g = group_rows<ODD, TEX>(p, lane, y0, z, wall);
             const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && g.bulk);
-            // x-segments: the shifted directions' halo pairs
-            const unsigned hvote = __ballot_sync(0xffffffffu, lane < Q && g.bulk && shift_of(wall) != 0);
             if (lane < Q) bulk_wait_read_all();  // this lane's store of the stage has read it
             __syncwarp();
             // one decision for the whole warp: lane 0's reading of the flag
@@ -649,8 +625,7 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
                 int x0 = 0, x1 = p.nx;
                 if (t.nseg > 1) group_xrange(t, gi, p.nx, x0, x1);
                 const size_t bytes = t.nseg > 1 ? (size_t)((x1 - x0 + 1) & ~1) * sizeof(T) : (size_t)k * t.row_bytes;
-                const size_t halo = t.nseg > 1 && seg_halo<T>(p.nx) ? (size_t)__popc(hvote) * 4 * sizeof(T) : 0;
-                if (lane == 0) mbar_expect_tx(full + st, (uint32_t)(__popc(vote) * bytes + halo));
+                if (lane == 0) mbar_expect_tx(full + st, (uint32_t)(__popc(vote) * bytes));
                 __syncwarp();
                 if (lane < Q && g.bulk) {
                     if (t.nseg > 1)
