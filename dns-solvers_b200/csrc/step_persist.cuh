@@ -349,8 +349,8 @@ __device__ __forceinline__ bool persist_grid_barrier(const PersistArgs &a, unsig
 }
 
 // ANYQ: some channel runs with a constant flow rate.  The launch bounds are
-// those of the 256-thread step form where the precision has one (FP32
-// without ANYQ: two blocks per SM; FP16: one block, no spills).
+// those of the dense step form where the precision has one (FP32 without
+// ANYQ: 256 threads, two blocks per SM; FP16: 256 threads, one block).
 template <typename T, bool ANYQ>
 __global__ void __launch_bounds__(TmaBounds<T, ANYQ>::threads, TmaBounds<T, ANYQ>::min_blocks)
     persist_batch_kernel(const PersistArgs a)

