@@ -73,6 +73,7 @@ void launch_tma_batch_lp(int precision, const ChannelLaunch *chans, int nchan, i
                          bool odd, cudaStream_t s);
 void launch_links_f64(const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s);
 void launch_links_lp(int precision, const LinksLaunch *tab, int n, int blocks, bool odd, cudaStream_t s);
+void launch_slab_tail(const StepArgs &a, int mode, double *slab_shift, int z0, int nzs, cudaStream_t s);
 }  // namespace dnslbm
 
 using namespace dnslbm;
@@ -136,6 +137,15 @@ struct dnslbm_ctx {
     int odd = 0;  // parity of the next step (1: populations are post-collision, swapped)
     long long done = 0;
     int slab_next = 0;  // next x of a state loaded in slabs
+    // wall-normal slab of a channel split over several GPUs
+    // (dnslbm_create_slab): the context holds fluid planes [z0, z0 + nz) of a
+    // channel of nz_all planes, each population array with one ghost plane
+    // on either side (pop_off elements from the array's start to plane 0)
+    int slab = 0, z0 = 0, nz_all = 0;
+    int wall_lo = 1, wall_hi = 1;
+    size_t pop_off = 0;
+    double *shift_all = nullptr;  // [2][nz_all][3] the channel's plane means (slab tail)
+    int tail_owed = -1;           // the slab tail the caller owes: 1 after a load, 0 after a step, -1 none
     char err[512] = {0};
 };
 
@@ -160,7 +170,7 @@ static int fail(dnslbm_ctx *c, int code, const char *fmt, ...)
 static StepArgs step_args(const dnslbm_ctx *c)
 {
     StepArgs p;
-    for (int a = 0; a < Q; ++a) p.pop[a] = (char *)c->popmem + (size_t)a * c->pstride * c->esize;
+    for (int a = 0; a < Q; ++a) p.pop[a] = (char *)c->popmem + ((size_t)a * c->pstride + c->pop_off) * c->esize;
     p.nx = c->nx;
     p.ny = c->ny;
     p.nz = c->nz;
@@ -186,13 +196,16 @@ static StepArgs step_args(const dnslbm_ctx *c)
     p.links = c->links;
     p.wait_ns = c->wait_ns;
     p.withhold_stage = 0;
+    p.wall_lo = c->wall_lo;
+    p.wall_hi = c->wall_hi;
+    p.tail = c->slab ? 0 : 1;
     return p;
 }
 
 static IoArgs io_args(const dnslbm_ctx *c)
 {
     IoArgs p;
-    for (int a = 0; a < Q; ++a) p.pop[a] = (char *)c->popmem + (size_t)a * c->pstride * c->esize;
+    for (int a = 0; a < Q; ++a) p.pop[a] = (char *)c->popmem + ((size_t)a * c->pstride + c->pop_off) * c->esize;
     p.nx = c->nx;
     p.ny = c->ny;
     p.nz = c->nz;
@@ -211,7 +224,8 @@ static void free_all(dnslbm_ctx *c)
                     c->plane_sums, c->logs,       c->step_ctr,      c->status,      c->plane_ctr,
                     c->total_ctr,  c->staging,    c->stat_partials, c->stat_planes, c->stat_mean,
                     c->band_of,    c->links,      c->plane_list,    c->d_llaunch,   c->stat_acc,
-                    c->out_lbf,    c->out_vel,    c->out_den,       c->out_stats,   c->quad_buf};
+                    c->out_lbf,    c->out_vel,    c->out_den,       c->out_stats,   c->quad_buf,
+                    c->shift_all};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &e : c->ev)
@@ -340,11 +354,20 @@ static cudaError_t upload_planes(dnslbm_ctx *c, const std::vector<int> *band = n
     return cudaMemcpy(c->plane_list, pl.data(), pl.size() * sizeof(int), cudaMemcpyHostToDevice);
 }
 
-extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
+// A whole channel (slab = 0) or the wall-normal slab [z0, z0 + nzs) of one
+// (slab = 1, dnslbm_create_slab).
+static int create_ctx(const dnslbm_deck *deck, int slab, int z0, int nzs, dnslbm_ctx **out)
 {
     dnslbm_ctx *c = nullptr;
     if (!deck || !out) return fail(c, DNSLBM_ERR_ARG, "null deck or output pointer");
     *out = nullptr;
+    if (slab) {
+        if (z0 < 0 || nzs < 2 || (long long)z0 + nzs > deck->zdv)
+            return fail(c, DNSLBM_ERR_ARG, "slab of planes [%d, %d) is not a range of at least 2 of the %d planes", z0,
+                        z0 + nzs, deck->zdv);
+        if (deck->bc_mode != DNSLBM_BC_REFERENCE)
+            return fail(c, DNSLBM_ERR_ARG, "slabs take the reference boundary mode (no solids inside the flow)");
+    }
     if (deck->xdv < 2 || deck->ydv < 2 || deck->zdv < 3)
         return fail(c, DNSLBM_ERR_ARG, "grid %dx%dx%d too small (need xdv,ydv >= 2, zdv >= 3)", deck->xdv, deck->ydv,
                     deck->zdv);
@@ -366,7 +389,12 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     if (c->deck.log_capacity == 0) c->deck.log_capacity = 4096;
     c->nx = deck->xdv;
     c->ny = deck->ydv;
-    c->nz = deck->zdv;
+    c->nz = slab ? nzs : deck->zdv;
+    c->slab = slab;
+    c->z0 = slab ? z0 : 0;
+    c->nz_all = deck->zdv;
+    c->wall_lo = c->z0 == 0;
+    c->wall_hi = c->z0 + c->nz == deck->zdv;
     c->nclean = c->nz;
     c->esize = deck->precision / 8;
     {
@@ -378,6 +406,13 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     }
     c->ncell = (size_t)c->pitch * c->ny * c->nz;
     const size_t align = 256 / c->esize;
+    if (slab) {
+        // a ghost plane on either side: plane -1 just below plane 0, plane
+        // nz just above plane nz-1; plane 0 starts on 256 bytes
+        const size_t plane = (size_t)c->pitch * c->ny;
+        c->pop_off = (plane + align - 1) / align * align;
+        c->ncell = c->pop_off + (size_t)(c->nz + 1) * plane;
+    }
     c->pstride = (c->ncell + align - 1) / align * align;
 
     int rc = DNSLBM_OK;
@@ -433,6 +468,10 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         }
         describe_kernel(c);
     }
+    if (slab && !c->use_tma) {
+        fail(c, DNSLBM_ERR_ARG, "slab contexts step with the row-pipelined kernel, which this grid cannot take");
+        return bail(DNSLBM_ERR_ARG);
+    }
     const size_t nblocks = (size_t)c->nz * c->slots;
 
     struct Alloc { void **p; size_t bytes; };
@@ -468,6 +507,14 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
         }
         cudaMemset(*a.p, 0, a.bytes);
     }
+    if (slab) {
+        const size_t bytes = (size_t)2 * c->nz_all * 3 * sizeof(double);
+        if (cudaMalloc((void **)&c->shift_all, bytes) != cudaSuccess) {
+            fail(c, DNSLBM_ERR_NOMEM, "cudaMalloc of %zu bytes failed", bytes);
+            return bail(DNSLBM_ERR_NOMEM);
+        }
+        cudaMemset(c->shift_all, 0, bytes);
+    }
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -495,6 +542,13 @@ extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out)
     (void)rc;
     *out = c;
     return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_create(const dnslbm_deck *deck, dnslbm_ctx **out) { return create_ctx(deck, 0, 0, 0, out); }
+
+extern "C" int dnslbm_create_slab(const dnslbm_deck *deck, int z0, int nzs, dnslbm_ctx **out)
+{
+    return create_ctx(deck, 1, z0, nzs, out);
 }
 
 extern "C" void dnslbm_destroy(dnslbm_ctx *c)
@@ -632,6 +686,22 @@ extern "C" int dnslbm_link_masks(int xdv, int ydv, int zdv, int bc_mode, const i
 static int apply_flags(dnslbm_ctx *c, const int8_t *fl /* [nx][ny][zd] */)
 {
     const int nx = c->nx, ny = c->ny, nz = c->nz;
+    std::vector<int8_t> view;
+    if (c->slab) {
+        // the whole channel's flags -> the slab's planes k = z0 .. z0 + nz + 1,
+        // a side that faces a neighbour slab reading as a no-slip wall plane
+        // (its wall-link bits are never used: plane_wall is 0 there)
+        const int zd_all = c->nz_all + 2, zd = nz + 2;
+        view.resize((size_t)nx * ny * zd);
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int kk = 0; kk < zd; ++kk) {
+                    const bool ghost = (kk == 0 && !c->wall_lo) || (kk == zd - 1 && !c->wall_hi);
+                    view[((size_t)x * ny + y) * zd + kk] =
+                        ghost ? (int8_t)-1 : fl[((size_t)x * ny + y) * zd_all + c->z0 + kk];
+                }
+        fl = view.data();
+    }
     FlagTables t;
     char err[256];
     const int brc = build_flag_tables(nx, ny, nz, c->deck.bc_mode == DNSLBM_BC_GENERAL, fl, t, err, sizeof err);
@@ -695,7 +765,7 @@ extern "C" int dnslbm_set_flags_periodic(dnslbm_ctx *c, const int8_t *flags)
 extern "C" int dnslbm_set_flags(dnslbm_ctx *c, const int *s)
 {
     if (!c || !s) return fail(c, DNSLBM_ERR_ARG, "null argument");
-    const int nx = c->nx, ny = c->ny, zd = c->nz + 2, yd = ny + 1;
+    const int nx = c->nx, ny = c->ny, zd = (c->slab ? c->nz_all : c->nz) + 2, yd = ny + 1;
     std::vector<int8_t> fl((size_t)nx * ny * zd);
     for (int x = 0; x < nx; ++x)
         for (int y = 0; y < ny; ++y)
@@ -707,6 +777,7 @@ extern "C" int dnslbm_set_flags(dnslbm_ctx *c, const int *s)
 }
 
 // initial reduction of a freshly set state: force and plane means of step 0
+// (a slab leaves its plane sums to the caller, who owes dnslbm_slab_tail)
 static int initial_reduce(dnslbm_ctx *c)
 {
     StepArgs p = step_args(c);
@@ -714,6 +785,7 @@ static int initial_reduce(dnslbm_ctx *c)
     else launch_reduce_lp(c->deck.precision, p, c->grid, c->block, c->stream);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->stream));
+    c->tail_owed = c->slab ? 1 : -1;
     return DNSLBM_OK;
 }
 
@@ -724,8 +796,10 @@ static int reset_counters(dnslbm_ctx *c)
     CK(cudaMemsetAsync(c->step_ctr, 0, sizeof(long long), c->stream));
     CK(cudaMemsetAsync(c->status, 0, 2 * sizeof(long long), c->stream));
     CK(cudaMemsetAsync(c->shift, 0, (size_t)2 * c->nz * 3 * sizeof(double), c->stream));
+    if (c->shift_all) CK(cudaMemsetAsync(c->shift_all, 0, (size_t)2 * c->nz_all * 3 * sizeof(double), c->stream));
     c->done = 0;
     c->odd = 0;
+    c->tail_owed = -1;
     return DNSLBM_OK;
 }
 
@@ -796,10 +870,20 @@ extern "C" int dnslbm_load_state_slab(dnslbm_ctx *c, int x0, int nxs, const doub
     return initial_reduce(c);
 }
 
+// Readers of the state need one; a slab is read between even numbers of
+// steps only (after an even step a reader gathers across the ghost planes,
+// which mirror the neighbour slabs only around an odd step).
+static int readable(dnslbm_ctx *c)
+{
+    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state loaded");
+    if (c->slab && c->odd) return fail(c, DNSLBM_ERR_STATE, "a slab is read after an even number of steps only");
+    return DNSLBM_OK;
+}
+
 extern "C" int dnslbm_store_state(dnslbm_ctx *c, double *state)
 {
     if (!c || !state) return fail(c, DNSLBM_ERR_ARG, "null argument");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state loaded");
+    if (int rc_ = readable(c)) return rc_;
     CK(cudaSetDevice(c->deck.device));
     IoArgs p = io_args(c);
     const size_t slab = (size_t)c->ny * (c->nz + 2) * Q;
@@ -903,6 +987,7 @@ extern "C" int dnslbm_step(dnslbm_ctx *c, long nsteps)
 {
     if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
     if (nsteps < 0) return fail(c, DNSLBM_ERR_ARG, "negative step count");
+    if (c->slab) return fail(c, DNSLBM_ERR_STATE, "a slab context steps with dnslbm_slab_step and dnslbm_slab_tail");
     if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state: call dnslbm_init_rest or dnslbm_load_state");
     CK(cudaSetDevice(c->deck.device));
     int rc = launch_steps(c, nsteps, false, nullptr, nullptr);
@@ -913,6 +998,7 @@ extern "C" int dnslbm_step(dnslbm_ctx *c, long nsteps)
 extern "C" int dnslbm_step_timed(dnslbm_ctx *c, long nsteps, double *ms_total, double *ms_even, double *ms_odd)
 {
     if (!c || !ms_total || !ms_even || !ms_odd) return fail(c, DNSLBM_ERR_ARG, "null argument");
+    if (c->slab) return fail(c, DNSLBM_ERR_STATE, "a slab context steps with dnslbm_slab_step and dnslbm_slab_tail");
     if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
     CK(cudaSetDevice(c->deck.device));
     *ms_even = *ms_odd = 0.0;
@@ -927,6 +1013,82 @@ extern "C" int dnslbm_step_timed(dnslbm_ctx *c, long nsteps, double *ms_total, d
     *ms_total = ms;
     return check_status(c);
 }
+
+// ---------------------------------------------------------------- slabs
+// A channel split into wall-normal slabs over several GPUs: the step kernel
+// of each slab leaves its plane sums; the caller gathers every slab's sums
+// in plane order and hands them to dnslbm_slab_tail, which runs the step
+// tail of the whole channel on each slab.  Around an odd step the caller
+// exchanges the ghost planes (dnslbm_slab_halo).
+static_assert(DNSLBM_SUM_N == NP, "the slab sums are the plane sums of the step kernels");
+
+extern "C" int dnslbm_slab_step(dnslbm_ctx *c)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    if (!c->slab) return fail(c, DNSLBM_ERR_STATE, "not a slab context (dnslbm_create_slab)");
+    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state: call dnslbm_init_rest or dnslbm_load_state");
+    if (c->tail_owed >= 0)
+        return fail(c, DNSLBM_ERR_STATE, "the tail of the last %s is owed first (dnslbm_slab_tail)",
+                    c->tail_owed ? "load" : "step");
+    CK(cudaSetDevice(c->deck.device));
+    int rc = launch_steps(c, 1, false, nullptr, nullptr);
+    if (rc) return rc;
+    c->tail_owed = 0;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_slab_sums(dnslbm_ctx *c, double **sums)
+{
+    if (!c || !sums) return fail(c, DNSLBM_ERR_ARG, "null argument");
+    if (!c->slab) return fail(c, DNSLBM_ERR_STATE, "not a slab context (dnslbm_create_slab)");
+    *sums = c->plane_sums;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_slab_tail(dnslbm_ctx *c, const double *sums_all)
+{
+    if (!c || !sums_all) return fail(c, DNSLBM_ERR_ARG, "null argument");
+    if (!c->slab) return fail(c, DNSLBM_ERR_STATE, "not a slab context (dnslbm_create_slab)");
+    if (c->tail_owed < 0) return fail(c, DNSLBM_ERR_STATE, "no step or load of this slab awaits its tail");
+    CK(cudaSetDevice(c->deck.device));
+    StepArgs a = step_args(c);
+    a.nz = c->nz_all;
+    a.plane_sums = const_cast<double *>(sums_all);
+    a.shift = c->shift_all;
+    launch_slab_tail(a, c->tail_owed, c->shift, c->z0, c->nz, c->stream);
+    CK(cudaGetLastError());
+    c->tail_owed = -1;
+    return DNSLBM_OK;
+}
+
+extern "C" int dnslbm_slab_status(dnslbm_ctx *c)
+{
+    if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
+    CK(cudaSetDevice(c->deck.device));
+    return check_status(c);
+}
+
+extern "C" int dnslbm_slab_halo(dnslbm_ctx *c, int side, void **ghost, void **edge, size_t *bytes)
+{
+    if (!c || !ghost || !edge || !bytes) return fail(c, DNSLBM_ERR_ARG, "null argument");
+    if (!c->slab) return fail(c, DNSLBM_ERR_STATE, "not a slab context (dnslbm_create_slab)");
+    if (side != 0 && side != 1) return fail(c, DNSLBM_ERR_ARG, "side %d is neither 0 (lower) nor 1 (upper)", side);
+    if (side == 0 ? c->wall_lo : c->wall_hi)
+        return fail(c, DNSLBM_ERR_ARG, "the %s face of this slab is a wall", side ? "upper" : "lower");
+    // directions leaving through the lower face (e_z = -1) and the upper one
+    static const int down[5] = {6, 12, 13, 16, 17}, up[5] = {5, 11, 14, 15, 18};
+    const StepArgs p = step_args(c);
+    const ptrdiff_t plane = (ptrdiff_t)c->ny * c->pitch;
+    for (int i = 0; i < 5; ++i) {
+        const int gs = side == 0 ? down[i] : up[i], es = side == 0 ? up[i] : down[i];
+        ghost[i] = (char *)p.pop[gs] + (side == 0 ? -plane : (ptrdiff_t)c->nz * plane) * (ptrdiff_t)c->esize;
+        edge[i] = (char *)p.pop[es] + (side == 0 ? 0 : (ptrdiff_t)(c->nz - 1) * plane) * (ptrdiff_t)c->esize;
+    }
+    *bytes = (size_t)plane * c->esize;
+    return DNSLBM_OK;
+}
+
+extern "C" void *dnslbm_stream(const dnslbm_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 extern "C" int dnslbm_set_wait_limit(dnslbm_ctx *c, double ms)
 {
@@ -980,7 +1142,7 @@ extern "C" int dnslbm_get_force(dnslbm_ctx *c, double *force)
 extern "C" int dnslbm_moments(dnslbm_ctx *c, double *vel, double *den)
 {
     if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (int rc_ = readable(c)) return rc_;
     if (!vel && !den) return DNSLBM_OK;
     CK(cudaSetDevice(c->deck.device));
     IoArgs p = io_args(c);
@@ -1004,7 +1166,7 @@ extern "C" int dnslbm_moments(dnslbm_ctx *c, double *vel, double *den)
 extern "C" int dnslbm_stats_accumulate(dnslbm_ctx *c)
 {
     if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (int rc_ = readable(c)) return rc_;
     CK(cudaSetDevice(c->deck.device));
     const double np = (double)c->nx * c->ny;
     IoArgs p = io_args(c);
@@ -1053,7 +1215,7 @@ extern "C" int dnslbm_stats_reset(dnslbm_ctx *c)
 extern "C" int dnslbm_statistics(dnslbm_ctx *c, double *out)
 {
     if (!c || !out) return fail(c, DNSLBM_ERR_ARG, "null argument");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (int rc_ = readable(c)) return rc_;
     CK(cudaSetDevice(c->deck.device));
     const int nz = c->nz, zd = nz + 2;
     const double np = (double)c->nx * c->ny;
@@ -1117,7 +1279,7 @@ static int out_alloc(dnslbm_ctx *c, double **p, size_t n)
 extern "C" int dnslbm_output_begin(dnslbm_ctx *c, double *state, double *vel, double *den, double *stats)
 {
     if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (int rc_ = readable(c)) return rc_;
     CK(cudaSetDevice(c->deck.device));
     const size_t cells = (size_t)c->nx * c->ny * (c->nz + 2);
     const int zd = c->nz + 2;
@@ -1180,7 +1342,7 @@ static void quadrant_finish(int zd, double n, const double *sums, double *quadra
 extern "C" int dnslbm_quadrant(dnslbm_ctx *c, double *quadrant, double *dquadrant, double *uw)
 {
     if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (int rc_ = readable(c)) return rc_;
     CK(cudaSetDevice(c->deck.device));
     const int zd = c->nz + 2;
     const size_t cells = (size_t)c->nx * c->ny * zd;
@@ -1260,7 +1422,7 @@ static cudaError_t correlations_of(const double *dvel, int nx, int ny, int zd, c
 extern "C" int dnslbm_correlations(dnslbm_ctx *c, double *xcorl, double *ycorl, double *uavg)
 {
     if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (int rc_ = readable(c)) return rc_;
     if (c->nx > correlation_max_line() || c->ny > correlation_max_line())
         return fail(c, DNSLBM_ERR_ARG, "correlation lines longer than %d cells", correlation_max_line());
     CK(cudaSetDevice(c->deck.device));
@@ -1334,7 +1496,7 @@ static cudaError_t spectra_of(const double *dvel, int nx, int ny, int zd, cudaSt
 extern "C" int dnslbm_spectra(dnslbm_ctx *c, double *ex, double *ey)
 {
     if (!c) return fail(c, DNSLBM_ERR_ARG, "null context");
-    if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
+    if (int rc_ = readable(c)) return rc_;
     CK(cudaSetDevice(c->deck.device));
     const int zd = c->nz + 2;
     const size_t cells = (size_t)c->nx * c->ny * zd;

@@ -47,7 +47,21 @@ struct StepArgs {
     // test switch (0 otherwise) that makes one block withhold a load
     unsigned long long wait_ns;
     int withhold_stage;
+    // wall-normal slab of a channel split over several GPUs: wall_lo /
+    // wall_hi say whether plane 0 / nz-1 lies next to the bottom / top wall
+    // (else next to a ghost plane, z = -1 / nz, that mirrors the neighbour
+    // slab); tail = 0 leaves the plane sums to the caller instead of running
+    // the step tail (whole channels: 1, 1, 1)
+    int wall_lo = 1, wall_hi = 1;
+    int tail = 1;
 };
+
+// -1: plane z lies next to the bottom wall, +1: next to the top wall, 0:
+// between fluid planes (a ghost plane of a slab included)
+__device__ __forceinline__ int plane_wall(const StepArgs &p, int z)
+{
+    return (z == 0 && p.wall_lo) ? -1 : ((z == p.nz - 1 && p.wall_hi) ? 1 : 0);
+}
 
 // Arguments of the state readers/writers (import, export, moments, stats).
 struct IoArgs {
@@ -313,7 +327,7 @@ __device__ __forceinline__ void plane_contribute(const StepArgs &a, double (&acc
     group_sync(nthreads);
     if (ticket != (unsigned)a.nz - 1) return;
     __threadfence();
-    step_tail(a, step, force_used, mode, smem, nthreads);
+    if (a.tail) step_tail(a, step, force_used, mode, smem, nthreads);
     if (threadIdx.x == 0) *a.total_ctr = 0;
     group_sync(nthreads);
 }

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(128, 4) step_f64_kernel(const StepArgs p)
     const double G = CONSTQ ? p.force[step & 1] : p.gx;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.z;
-    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const int wall = plane_wall(p, z);
     const double c0 = p.shift[(size_t)(step & 1) * p.nz * 3 + z * 3 + 0];
     const double c1 = p.shift[(size_t)(step & 1) * p.nz * 3 + z * 3 + 1];
     const double c2 = p.shift[(size_t)(step & 1) * p.nz * 3 + z * 3 + 2];
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(128) reduce_f64_odd_kernel(const StepArgs p)
     const long long step = *p.step_ctr;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.z;
-    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const int wall = plane_wall(p, z);
     double acc[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) acc[i] = 0.0;
@@ -206,6 +206,33 @@ void launch_reduce_f64_odd(const StepArgs &p, dim3 grid, dim3 block, int tex, cu
 {
     if (tex) reduce_f64_odd_kernel<1><<<grid, block, 0, s>>>(p);
     else reduce_f64_odd_kernel<0><<<grid, block, 0, s>>>(p);
+}
+
+// Step tail of one wall-normal slab of a channel split over several GPUs
+// (one block).  `a` describes the whole channel: nz planes, the plane sums
+// of all slabs gathered in plane order, the context's copy of the whole
+// channel's plane means.  The tail is the one a whole-channel step runs
+// (step_tail: logs, force, plane means; identical on every slab, which all
+// hold the same gathered sums); then the slab's planes [z0, z0 + nzs) of
+// the new plane means go to its own shift array ([2][nzs][3]), which its
+// step kernel reads.  mode 0 after a step, 1 after a state load.
+__global__ void __launch_bounds__(256) slab_tail_kernel(const StepArgs a, int mode, double *slab_shift, int z0,
+                                                        int nzs)
+{
+    __shared__ double smem[32 * NP];
+    const long long step = __ldcg(a.step_ctr);
+    const double force_used = __ldcg(a.force + (step & 1));
+    step_tail(a, step, force_used, mode, smem, blockDim.x);
+    __syncthreads();
+    const int par = (int)((mode == 0 ? step + 1 : step) & 1);
+    const double *src = a.shift + (size_t)par * a.nz * 3 + (size_t)z0 * 3;
+    double *dst = slab_shift + (size_t)par * nzs * 3;
+    for (int i = threadIdx.x; i < nzs * 3; i += blockDim.x) dst[i] = __ldcg(src + i);
+}
+
+void launch_slab_tail(const StepArgs &a, int mode, double *slab_shift, int z0, int nzs, cudaStream_t s)
+{
+    slab_tail_kernel<<<1, 256, 0, s>>>(a, mode, slab_shift, z0, nzs);
 }
 
 }  // namespace dnslbm

@@ -253,7 +253,7 @@ __device__ __forceinline__ void links_pass_body(const LinksLaunch &L, int blk)
     const int pi = blk / per_plane, r = blk - pi * per_plane;
     const int by = r / L.xblocks, bx = r - by * L.xblocks;
     const int z = L.planes[pi];
-    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const int wall = plane_wall(p, z);
     const long long step = *p.step_ctr;
     const double G = CONSTQ ? p.force[step & 1] : p.gx;
     const double *sh = p.shift + (size_t)(step & 1) * p.nz * 3 + z * 3;

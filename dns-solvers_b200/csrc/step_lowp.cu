@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(128, 4) step_lp_kernel(const StepArgs p)
     const float G = (float)Gd;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.z;
-    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const int wall = plane_wall(p, z);
     const double *sh = p.shift + (size_t)(step & 1) * p.nz * 3 + z * 3;
     const double c0 = sh[0], c1 = sh[1], c2 = sh[2];
     double acc[NP];

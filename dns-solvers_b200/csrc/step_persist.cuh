@@ -128,7 +128,7 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
         if (*s_abort || H.item < 0 || (ODD && H.it.kind == 1) || lane >= Q) return;
         const ChannelLaunch &L = chans[H.it.chan];
         const int k = min(L.t.k, L.p.ny - H.y0);
-        const int wall = H.z == 0 ? -1 : (H.z == L.p.nz - 1 ? 1 : 0);
+        const int wall = plane_wall(L.p, H.z);
         const GroupRows gr = L.textured ? group_rows<ODD, 1>(L.p, lane, H.y0, H.z, wall)
                                         : group_rows<ODD, 0>(L.p, lane, H.y0, H.z, wall);
         const size_t dir_bytes = (size_t)L.t.dir_elems * sizeof(T);
@@ -170,7 +170,7 @@ __device__ __forceinline__ void persist_producer(const PersistArgs &a, int s, in
                 int z, y0;
                 group_origin(L.t, it.first + g, z, y0);
                 const int k = min(L.t.k, L.p.ny - y0);
-                const int wall = z == 0 ? -1 : (z == L.p.nz - 1 ? 1 : 0);
+                const int wall = plane_wall(L.p, z);
                 GroupRows gr{};
                 if (lane < Q)
                     gr = tex ? group_rows<ODD, 1>(L.p, lane, y0, z, wall) : group_rows<ODD, 0>(L.p, lane, y0, z, wall);
@@ -216,7 +216,7 @@ __device__ __forceinline__ void persist_links(const StepArgs &p, T *sb, int dstr
                                               const double (&sh)[3], double (&acc)[NP], int nc)
 {
     const int nx = p.nx;
-    const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+    const int wall = plane_wall(p, z);
     for (int c = threadIdx.x; c < k * nx; c += nc) {
         const int j = c / nx, x = c - j * nx, y = y0 + j;
         float racc[NP];

@@ -184,7 +184,7 @@ __device__ __forceinline__ void copy_group(const StepArgs &p, const TmaArgs &t, 
     const int ny = p.ny;
     const size_t rb = (size_t)t.row_bytes;
     auto one = [&](int ysrc, int j, int nrows) {
-        T *gp = static_cast<T *>(p.pop[g.slot]) + (size_t)(g.zz * ny + ysrc) * p.pitch;
+        T *gp = static_cast<T *>(p.pop[g.slot]) + (ptrdiff_t)(g.zz * ny + ysrc) * p.pitch;
         unsigned char *sp = sdir + (size_t)j * rb;
         if (to_smem) bulk_g2s(sp, gp, (uint32_t)(nrows * rb), bar);
         else bulk_s2g(gp, sp, (uint32_t)(nrows * rb));
@@ -218,7 +218,7 @@ __device__ __forceinline__ void copy_segment(const StepArgs &p, const GroupRows 
     const int ny = p.ny, L = x1 - x0, Lp = (L + 1) & ~1;
     int y = g.y_first;
     y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
-    T *row = static_cast<T *>(p.pop[g.slot]) + (size_t)(g.zz * ny + y) * p.pitch;
+    T *row = static_cast<T *>(p.pop[g.slot]) + (ptrdiff_t)(g.zz * ny + y) * p.pitch;
     if (to_smem) {
         bulk_g2s(sdir + 2 * sizeof(T), row + x0, (uint32_t)(Lp * sizeof(T)), bar);
         return;
@@ -263,7 +263,7 @@ __device__ __forceinline__ void tma_group(const StepArgs &p, T *sb, int dstride,
         auto shifted_ptr = [&](int A, int xs) {
             int yy = y + lat_ey(A);
             yy = yy < 0 ? yy + p.ny : (yy >= p.ny ? yy - p.ny : yy);
-            return static_cast<T *>(p.pop[A]) + ((size_t)(z + lat_ez(A)) * p.ny + yy) * pitch + xs;
+            return static_cast<T *>(p.pop[A]) + ((ptrdiff_t)(z + lat_ez(A)) * p.ny + yy) * pitch + xs;
         };
         unsigned bits = 0x1fu;
         if (TEXTURED && WALL != 0) bits = p.wallmask[(size_t)(WALL > 0) * nx * p.ny + (size_t)y * nx + x];
@@ -578,7 +578,7 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             int z, y0;
             group_origin(t, gi, z, y0);
             const int k = min(t.k, p.ny - y0);
-            const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+            const int wall = plane_wall(p, z);
             if (lane < Q && !*abort) {
                 const GroupRows g = group_rows<ODD, TEX>(p, lane, y0, z, wall);
                 if (g.bulk) {
@@ -598,7 +598,7 @@ __device__ __forceinline__ void tma_producer(const StepArgs &p, const TmaArgs &t
             int z, y0;
             group_origin(t, gi, z, y0);
             const int k = min(t.k, p.ny - y0);
-            const int wall = z == 0 ? -1 : (z == p.nz - 1 ? 1 : 0);
+            const int wall = plane_wall(p, z);
             GroupRows g{};
             if (lane < Q) g = group_rows<ODD, TEX>(p, lane, y0, z, wall);
             const unsigned vote = __ballot_sync(0xffffffffu, lane < Q && g.bulk);
@@ -663,15 +663,16 @@ template <typename T, bool ODD, bool CONSTQ, bool TXT>
 __device__ __forceinline__ void consume_group(const StepArgs &p, const LpParams &lk, T *sb, int dstride, int y0, int k,
                                               int z, double G, const double *sh, double (&acc)[NP], int nc)
 {
+    const int wall = plane_wall(p, z);
     if constexpr (std::is_same<T, double>::value) {
-        if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
-        else if (z == p.nz - 1) tma_group<T, ODD, CONSTQ, TXT, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        if (wall < 0) tma_group<T, ODD, CONSTQ, TXT, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
+        else if (wall > 0) tma_group<T, ODD, CONSTQ, TXT, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
         else tma_group<T, ODD, CONSTQ, TXT, 0>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
     } else {
-        if (z == 0) {
+        if (wall < 0) {
             if (TXT) tma_group<T, ODD, CONSTQ, true, -1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
             else tma_group2<T, ODD, CONSTQ, -1>(p, lk, sb, dstride, k, sh, acc, nc);
-        } else if (z == p.nz - 1) {
+        } else if (wall > 0) {
             if (TXT) tma_group<T, ODD, CONSTQ, true, 1>(p, sb, dstride, y0, k, z, G, sh, acc, nc);
             else tma_group2<T, ODD, CONSTQ, 1>(p, lk, sb, dstride, k, sh, acc, nc);
         } else {
@@ -734,8 +735,9 @@ __device__ __forceinline__ void tma_step_body(const StepArgs &p, const TmaArgs &
                 group_xrange(t, gi, p.nx, x0, x1);
                 constexpr bool TXT = TEX != 0;
                 const double *sh = shift_now + z * 3;
-                if (z == 0) tma_group<T, ODD, CONSTQ, TXT, -1, true>(p, sb, dstride, y0, 1, z, G, sh, acc, nc, x0, x1);
-                else if (z == p.nz - 1)
+                const int wall = plane_wall(p, z);
+                if (wall < 0) tma_group<T, ODD, CONSTQ, TXT, -1, true>(p, sb, dstride, y0, 1, z, G, sh, acc, nc, x0, x1);
+                else if (wall > 0)
                     tma_group<T, ODD, CONSTQ, TXT, 1, true>(p, sb, dstride, y0, 1, z, G, sh, acc, nc, x0, x1);
                 else tma_group<T, ODD, CONSTQ, TXT, 0, true>(p, sb, dstride, y0, 1, z, G, sh, acc, nc, x0, x1);
             } else {

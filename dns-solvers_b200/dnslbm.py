@@ -107,6 +107,15 @@ def lib():
     L.dnslbm_batch_kernel.restype = ctypes.c_char_p
     L.dnslbm_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     L.dnslbm_batch_test_withhold_load.argtypes = [vp, ctypes.c_double]
+    L.dnslbm_create_slab.argtypes = [ctypes.POINTER(Deck), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.dnslbm_slab_step.argtypes = [vp]
+    L.dnslbm_slab_sums.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.dnslbm_slab_tail.argtypes = [vp, vp]
+    L.dnslbm_slab_status.argtypes = [vp]
+    L.dnslbm_slab_halo.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                   ctypes.POINTER(ctypes.c_size_t)]
+    L.dnslbm_stream.argtypes = [vp]
+    L.dnslbm_stream.restype = vp
     L.dnslbm_host_alloc.argtypes = [ctypes.c_size_t]
     L.dnslbm_host_alloc.restype = vp
     L.dnslbm_host_free.argtypes = [vp]
@@ -318,6 +327,76 @@ class Channel:
 
     def sync(self):
         self._ck(self.L.dnslbm_sync(self.h))
+
+
+class Slab(Channel):
+    """Wall-normal planes [z0, z0 + nzs) of a channel of zdv planes, on one
+    GPU (dnslbm_create_slab).  States (load/store, moments, statistics) are
+    the slab's planes, arrays of shape (xdv, ydv, nzs + 2, 19); flags are the
+    whole channel's.  It steps with its neighbours through a SlabGroup or a
+    HaloExchange (slabs.py), never alone with step()."""
+
+    SUM_N = 8  # doubles per plane of the slab sums (DNSLBM_SUM_N)
+
+    def __init__(self, xdv, ydv, zdv, z0, nzs, omega, ubulk=0.0, gx=0.0, force_mode=CONST_G, precision=F64,
+                 log_capacity=0, device=0):
+        self.L = lib()
+        self.channel_shape = (xdv, ydv, zdv)
+        self.shape = (xdv, ydv, nzs)
+        self.z0, self.nzs, self.device = z0, nzs, device
+        d = Deck(xdv, ydv, zdv, omega, ubulk, gx, force_mode, precision, BC_REFERENCE, log_capacity, device)
+        h = ctypes.c_void_p()
+        rc = self.L.dnslbm_create_slab(ctypes.byref(d), z0, nzs, ctypes.byref(h))
+        if rc:
+            raise DnsLbmError(rc, self.L.dnslbm_last_error(None).decode())
+        self.h = h
+        self.deck = d
+        self.walls = (z0 == 0, z0 + nzs == zdv)
+
+    def set_flags(self, flags):
+        """The whole channel's flags: int8 (xdv, ydv, zdv+2) or the
+        reference's V.s (xdv+1, ydv+1, zdv+2)."""
+        x, y, z = self.channel_shape
+        if flags.dtype == np.int8:
+            f = np.ascontiguousarray(flags)
+            assert f.shape == (x, y, z + 2)
+            self._ck(self.L.dnslbm_set_flags_periodic(self.h, f.ctypes.data_as(ctypes.POINTER(ctypes.c_int8))))
+        else:
+            f = np.ascontiguousarray(flags, np.int32)
+            assert f.shape == (x + 1, y + 1, z + 2)
+            self._ck(self.L.dnslbm_set_flags(self.h, f.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+
+    def part(self, whole):
+        """The slab's planes k = z0 .. z0+nzs+1 of a whole-channel array
+        (state, vel, den: axis 2 is k)."""
+        return np.ascontiguousarray(whole[:, :, self.z0:self.z0 + self.nzs + 2])
+
+    def kernel_step(self):
+        self._ck(self.L.dnslbm_slab_step(self.h))
+
+    def sums_ptr(self):
+        p = ctypes.c_void_p()
+        self._ck(self.L.dnslbm_slab_sums(self.h, ctypes.byref(p)))
+        return p.value
+
+    def tail(self, sums_all_ptr):
+        self._ck(self.L.dnslbm_slab_tail(self.h, ctypes.c_void_p(sums_all_ptr)))
+
+    def status(self):
+        self._ck(self.L.dnslbm_slab_status(self.h))
+
+    def halo(self, side):
+        """(ghost pointers[5], edge pointers[5], bytes per plane) of face
+        `side` (0 lower, 1 upper), or None on a wall face."""
+        if self.walls[side]:
+            return None
+        g, e, n = (ctypes.c_void_p * 5)(), (ctypes.c_void_p * 5)(), ctypes.c_size_t()
+        self._ck(self.L.dnslbm_slab_halo(self.h, side, g, e, ctypes.byref(n)))
+        return [v for v in g], [v for v in e], n.value
+
+    @property
+    def stream(self):
+        return self.L.dnslbm_stream(self.h)
 
 
 class _Borrowed(Channel):

@@ -147,6 +147,54 @@ int dnslbm_logs(dnslbm_ctx *ctx, long first, long count, double *out);
 /* Force the next step will use (V.force). */
 int dnslbm_get_force(dnslbm_ctx *ctx, double *force);
 
+/* ---- A channel split over several GPUs: wall-normal slabs ----
+ * Replaces the reference's domain decomposition (the MPI cartesian grid of
+ * dns-const-q-xycut.c:63-125) and its halo exchange (the persistent
+ * requests of :363-376 started in xcomputations.c:222-289,435-555) for a
+ * decomposition across the wall-normal planes: a slab holds whole planes,
+ * which are contiguous in each population array, so its halo is five whole
+ * planes per face and its plane statistics stay its own.  One context per
+ * GPU (one process per GPU); the exchange is the caller's (NCCL, CUDA-aware
+ * MPI, device copies) through the pointers below, on the context's stream.
+ *
+ * dnslbm_create_slab: fluid planes [z0, z0+nzs) (nzs >= 2) of the channel
+ * `deck` describes (deck->zdv planes), the reference boundary mode only.
+ * Flags (dnslbm_set_flags / _periodic) are the whole channel's; states
+ * (dnslbm_load_state / dnslbm_store_state and the other readers) are the
+ * slab's planes in the lbf layout with zd = nzs + 2 (planes k = z0 .. z0 +
+ * nzs + 1 of the whole lbf, the first and last ignored on load), read only
+ * after an even number of steps.  dnslbm_step refuses a slab; per step:
+ *   1. before an odd step (dnslbm_steps_done odd): every slab fills its
+ *      ghost planes from its neighbours (ghost <- neighbour's edge);
+ *   2. dnslbm_slab_step: the step kernel; it leaves the slab's plane sums
+ *      (nzs * DNSLBM_SUM_N doubles, dnslbm_slab_sums) on the device;
+ *   3. after an odd step: every slab sends its ghost planes back
+ *      (neighbour's edge <- ghost);
+ *   4. the caller gathers all slabs' sums in plane order (deck->zdv *
+ *      DNSLBM_SUM_N doubles in device memory) and calls dnslbm_slab_tail:
+ *      logs, constant-Q force and plane means of the whole channel, the same
+ *      on every slab.  A load or dnslbm_init_rest also owes one
+ *      dnslbm_slab_tail (steps 2 and 4 without the step).
+ * With constant g the populations are bit-identical to the whole channel
+ * stepped by one context.  No call of the sequence synchronises the host;
+ * dnslbm_slab_status waits for the stream and reports NaN / timeouts. */
+#define DNSLBM_SUM_N 8
+int dnslbm_create_slab(const dnslbm_deck *deck, int z0, int nzs, dnslbm_ctx **out);
+int dnslbm_slab_step(dnslbm_ctx *ctx);
+int dnslbm_slab_sums(dnslbm_ctx *ctx, double **sums);
+int dnslbm_slab_tail(dnslbm_ctx *ctx, const double *sums_all);
+int dnslbm_slab_status(dnslbm_ctx *ctx);
+/* Device pointers of the five population planes exchanged across the lower
+ * (side 0) or upper (side 1) face, in a fixed direction order: ghost[i] of
+ * the ghost plane beyond the face, edge[i] of the slab's own plane at the
+ * face; *bytes per plane.  Pairing: a slab's ghost on side s mirrors its
+ * neighbour's edge on side 1-s, entry for entry.  DNSLBM_ERR_ARG on a face
+ * next to a wall. */
+int dnslbm_slab_halo(dnslbm_ctx *ctx, int side, void **ghost, void **edge, size_t *bytes);
+/* The context's CUDA stream (a cudaStream_t): every call of the context is
+ * ordered on it. */
+void *dnslbm_stream(const dnslbm_ctx *ctx);
+
 /* statistics.c:3-183 of the current state: out[9*zd]. */
 int dnslbm_statistics(dnslbm_ctx *ctx, double *out);
 /* Time averages of the plane statistics kept on the device: each
