@@ -997,14 +997,15 @@ extern "C" int dnslbm_step(dnslbm_ctx *c, long nsteps)
 
 extern "C" int dnslbm_step_timed(dnslbm_ctx *c, long nsteps, double *ms_total, double *ms_even, double *ms_odd)
 {
-    if (!c || !ms_total || !ms_even || !ms_odd) return fail(c, DNSLBM_ERR_ARG, "null argument");
+    if (!c || !ms_total || (!ms_even) != (!ms_odd)) return fail(c, DNSLBM_ERR_ARG, "null argument");
     if (c->slab) return fail(c, DNSLBM_ERR_STATE, "a slab context steps with dnslbm_slab_step and dnslbm_slab_tail");
     if (!c->have_state) return fail(c, DNSLBM_ERR_STATE, "no state");
     CK(cudaSetDevice(c->deck.device));
-    *ms_even = *ms_odd = 0.0;
+    const bool per_launch = ms_even != nullptr;  // an event pair around every launch
+    if (per_launch) *ms_even = *ms_odd = 0.0;
     if (nsteps <= 0) return fail(c, DNSLBM_ERR_ARG, "timed run needs at least one step");
     CK(cudaEventRecord(c->ev[0], c->stream));
-    int rc = launch_steps(c, nsteps, true, ms_even, ms_odd);
+    int rc = launch_steps(c, nsteps, per_launch, ms_even, ms_odd);
     if (rc) return rc;
     CK(cudaEventRecord(c->ev[1], c->stream));
     CK(cudaEventSynchronize(c->ev[1]));

@@ -765,6 +765,13 @@ __global__ void __launch_bounds__(WIDE ? kTmaMaxThreads : TmaBounds<T, CONSTQ>::
     step_tma_kernel(const StepArgs p, const TmaArgs t)
 {
     extern __shared__ __align__(128) unsigned char tma_smem[];
+    // Launched with programmatic stream serialization (launch_tma): a block
+    // may start on an SM that the previous step's grid has left while that
+    // grid still runs.  Before anything else it waits for the previous grid
+    // to complete with its memory visible; then it lets the next step's grid
+    // be scheduled, whose blocks wait here in turn.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if constexpr (WIDE || TmaBounds<T, CONSTQ>::has_dense) tma_step_body<T, ODD, CONSTQ, TEX>(p, t, blockIdx.x, tma_smem);
 }
 
@@ -845,10 +852,25 @@ void launch_tma(const StepArgs &p, const TmaArgs &t, int grid, int threads, size
 {
     const bool q = p.const_q != 0;
     const bool wide = q ? tma_wide<T, true>(threads) : tma_wide<T, false>(threads);
+    // programmatic stream serialization: the launch and the blocks' start
+    // overlap the end of the previous step (the kernel orders itself after
+    // it with griddepcontrol.wait); the grid is never larger than what is
+    // resident at once, so a waiting block never keeps one of the previous
+    // grid's blocks from running
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
 #define L(O, C, X)                                                                            \
     do {                                                                                      \
-        if (wide || !TmaBounds<T, C>::has_dense) step_tma_kernel<T, O, C, X, true><<<grid, threads, smem, s>>>(p, t); \
-        else step_tma_kernel<T, O, C, X, false><<<grid, threads, smem, s>>>(p, t);           \
+        if (wide || !TmaBounds<T, C>::has_dense) cudaLaunchKernelEx(&cfg, step_tma_kernel<T, O, C, X, true>, p, t); \
+        else cudaLaunchKernelEx(&cfg, step_tma_kernel<T, O, C, X, false>, p, t);             \
     } while (0)
 #define LX(O, C) do { if (tex) L(O, C, 1); else L(O, C, 0); } while (0)
     if (odd) {

@@ -206,8 +206,13 @@ class Channel:
     def step(self, n=1):
         self._ck(self.L.dnslbm_step(self.h, n))
 
-    def step_timed(self, n):
+    def step_timed(self, n, per_launch=True):
+        """(total ms, even-launch ms, odd-launch ms) of n steps; per_launch
+        False times the whole run only (even/odd None)."""
         t, e, o = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        if not per_launch:
+            self._ck(self.L.dnslbm_step_timed(self.h, n, ctypes.byref(t), None, None))
+            return t.value, None, None
         self._ck(self.L.dnslbm_step_timed(self.h, n, ctypes.byref(t), ctypes.byref(e), ctypes.byref(o)))
         return t.value, e.value, o.value
 

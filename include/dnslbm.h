@@ -284,7 +284,9 @@ int dnslbm_spectra_vel(const double *vel, int xdv, int ydv, int zdv, int device,
 
 /* Timing support for benchmarks: advance nsteps like dnslbm_step and return
  * CUDA-event times on the context's stream: total, and the summed device
- * time of the two step kernels (even / odd parity launches). */
+ * time of the two step kernels (even / odd parity launches).  With ms_even
+ * and ms_odd both NULL only the total is taken (no event between launches,
+ * which lets each launch overlap the end of the previous one). */
 int dnslbm_step_timed(dnslbm_ctx *ctx, long nsteps, double *ms_total, double *ms_even, double *ms_odd);
 /* Autotuner: choose the step kernel's launch shape (per-thread kernel, or the
  * row-pipelined kernel's rows per stage group, stages in flight and consumer
