@@ -1755,6 +1755,7 @@ struct dnslbm_batch {
     int pgrid = 0;                      // its blocks (all resident)
     size_t pstage = 0, psmem = 0;       // bytes of one stage, dynamic shared memory
     std::vector<BatchItem> items;       // the items of one step, largest first
+    int items_per_block = 4;            // items per resident block and step the items are cut for
     std::vector<BatchItem> items_uploaded;
     BatchItem *d_items = nullptr;
     size_t d_items_cap = 0;
@@ -1878,7 +1879,9 @@ static void batch_layout(dnslbm_batch *b)
 
 // The items of one step of the persistent kernel: each plane of each
 // channel cut into runs of whole row groups of about W cells, W chosen so
-// that every resident block takes about four items per step; kind 1 for the
+// that every resident block takes about items_per_block items per step (more
+// and smaller items even out the blocks' ends of a step, at a cost per
+// item; the batch autotuner picks the count); kind 1 for the
 // planes with link masks (the channel's plane list holds them after the
 // others, so the group numbering covers them).  Largest first, so the last
 // items taken are the small ones.  An item's slot is its index within its
@@ -1887,7 +1890,7 @@ static void persist_items(dnslbm_batch *b)
 {
     double total = 0;
     for (auto *c : b->ch) total += (double)c->nx * c->ny * c->nz;
-    const double W = std::max(1.0, total / (4.0 * std::max(1, b->pgrid)));
+    const double W = std::max(1.0, total / ((double)b->items_per_block * std::max(1, b->pgrid)));
     std::vector<BatchItem> it;
     std::vector<double> cells;
     for (int ci = 0; ci < (int)b->ch.size(); ++ci) {
@@ -2338,6 +2341,22 @@ extern "C" int dnslbm_batch_autotune(dnslbm_batch *b, int steps, char *report, s
                 ++ncand;
                 if (ms < best) best = ms, bb = budget, bs = st, bc = cons;
             }
+    // the persistent kernel: how finely each step's work is cut, at the best shape
+    if (b->persistent) {
+        int bi = b->items_per_block;
+        for (int ipb : {2, 8, 16}) {
+            b->items_per_block = ipb;
+            if (batch_configure(b, bb, bs, bc)) continue;
+            int rc = DNSLBM_OK;
+            for (auto *c : b->ch)
+                if ((rc = dnslbm_init_rest(c))) return bfail(b, rc, "%s", c->err);
+            double ms = 0;
+            if ((rc = batch_run(b, 2, nullptr)) || (rc = batch_run(b, steps, &ms))) return rc;
+            ++ncand;
+            if (ms < best) best = ms, bi = ipb;
+        }
+        b->items_per_block = bi;
+    }
     // leave the channels as created: no state, counters clear
     for (auto *c : b->ch) {
         int rc = reset_counters(c);
