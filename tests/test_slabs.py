@@ -215,3 +215,73 @@ def test_slab_state_is_read_between_even_steps():
         g.store_state()
     finally:
         g.close()
+
+
+@pytest.mark.gpu
+def test_slab_readers_match_the_whole_channel():
+    """Moments and plane statistics of each slab are the whole channel's
+    rows for the slab's planes."""
+    import dnslbm
+    nx, ny, nz, omega, g = 32, 12, 12, 1.7, 2e-5
+    fl = inputs.flags_longitudinal(nx, ny, nz, 2, 2)
+    s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 31)
+    with dnslbm.Channel(nx, ny, nz, omega, gx=g, device=0) as ch:
+        ch.set_flags(fl)
+        ch.load_state(s0)
+        ch.step(6)
+        vel, den = ch.moments()
+        stats = ch.statistics()
+    grp = slabs.SlabGroup([dnslbm.Slab(nx, ny, nz, z0, n, omega, gx=g, device=0) for z0, n in [(0, 5), (5, 7)]])
+    try:
+        grp.set_flags(fl)
+        grp.load_state(s0)
+        grp.step(6)
+        for s in grp.slabs:
+            v, d = s.moments()
+            st = s.statistics()
+            k = slice(s.z0 + 1, s.z0 + s.nzs + 1)
+            np.testing.assert_array_equal(v[:, :, 1:-1], vel[:, :, k])
+            np.testing.assert_array_equal(d[:, :, 1:-1], den[:, :, k])
+            np.testing.assert_allclose(st[:, 1:-1], stats[:, k], rtol=1e-12, atol=1e-16)
+    finally:
+        grp.close()
+
+
+DIST_ONE_RANK = """
+import sys, os, datetime
+sys.path.insert(0, {pkg!r})
+import numpy as np, torch, torch.distributed as dist
+import dnslbm, inputs, slabs
+dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=60),
+                        device_id=torch.device("cuda:0"))
+nx, ny, nz, omega, g = 32, 12, 10, 1.7, 2e-5
+fl = inputs.flags_longitudinal(nx, ny, nz, 2, 2)
+s0 = inputs.laminar_state(nx, ny, nz, 0.08, 0.1, 17)
+with dnslbm.Channel(nx, ny, nz, omega, gx=g, device=0) as ch:
+    ch.set_flags(fl); ch.load_state(s0); ch.step(8); want = ch.store_state(); wl = ch.logs()
+s = dnslbm.Slab(nx, ny, nz, 0, nz, omega, gx=g, device=0)
+s.set_flags(fl)
+s.load_state(s.part(s0))
+ds = slabs.DistributedSlab(s)
+ds.after_load()
+ds.step(8)
+got = s.store_state()
+assert np.array_equal(got[:, :, 1:-1], want[:, :, 1:-1])
+assert np.allclose(s.logs(), wl, rtol=1e-11, atol=1e-14)
+s.close()
+dist.destroy_process_group()
+print("ok")
+"""
+
+
+@pytest.mark.gpu
+def test_distributed_slab_one_rank_nccl():
+    """DistributedSlab on a one-rank NCCL group (this run has one GPU): the
+    sums gather and the tail run on the slab's own stream through NCCL, and
+    the channel steps bit-identically to one context."""
+    code = DIST_ONE_RANK.format(pkg=os.path.join(ROOT, "dns-solvers_b200"))
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()),
+               NCCL_NVLS_ENABLE="0")
+    p = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-3000:]
+    assert p.stdout.split()[-1:] == ["ok"], p.stdout[-500:]  # NCCL may print its version first
