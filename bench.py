@@ -40,6 +40,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "dns-solvers_b200"))
 METRIC = "MLUPS & % HBM roofline: FP64 vs FP32/FP16-storage, at stated stats error"
 FALLBACK_HBM_GBS = 6650.0
+# steps each candidate launch shape is timed for: launch shapes within a
+# percent of each other change places over 6 steps
+TUNE_STEPS = 16
 
 
 def parse():
@@ -368,7 +371,7 @@ def run_ours(args):
     ch = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, ubulk=wl.ubulk, gx=wl.gx, force_mode=dnslbm.CONST_G,
                         precision=args.precision, bc_mode=bc, device=dev)
     ch.set_flags(flags)
-    tune = None if args.no_autotune else ch.autotune()
+    tune = None if args.no_autotune else ch.autotune(TUNE_STEPS)
     load(ch)
     ch.step_timed(args.warmup)
     d.barrier()
@@ -413,7 +416,7 @@ def run_ours(args):
             c2 = dnslbm.Channel(wl.nx, wl.ny, wl.nz, wl.omega, ubulk=wl.ubulk, gx=wl.gx,
                                 force_mode=dnslbm.CONST_G, precision=prec, bc_mode=bc, device=dev)
             c2.set_flags(flags)
-            tune2 = None if args.no_autotune else c2.autotune()
+            tune2 = None if args.no_autotune else c2.autotune(TUNE_STEPS)
             load(c2)
             c2.step_timed(args.warmup)
             t2 = c2.step_timed(args.steps, per_launch=False)[0]
